@@ -1,0 +1,151 @@
+"""Seeded synthetic Cholesky-MP2 inputs.
+
+The recipe (used for every synthetic workload of this package):
+
+* Cholesky vectors ``L^Q = s_Q * G^Q`` with ``G^Q = (X + X^T)/2``,
+  ``X ~ N(0,1)`` (N x N), and ``s_Q = 10**(-6 Q / M)`` for ``Q = 0..M-1``.
+  Stored as the reference's ``CholeskyERI`` does: M vectors of length N*N,
+  index ``mu*N + nu`` (reference include/mshqc/integrals/cholesky_eri.h:81, :89-91).
+* MO coefficients ``C``: the Q factor of the QR decomposition of a Gaussian
+  N x N matrix (column-major on the C-ABI, Eigen convention).
+* Occupied energies uniform in [-2.0, -0.3] Eh with the 4 lowest set to
+  -20 Eh; virtual energies log-uniform in [0.05, 5] Eh; sorted ascending so
+  that the first ``nocc`` columns of C are the occupied orbitals
+  (``leftCols(nocc)`` in reference src/mp2/cholesky_rmp2.cc:77-78).
+* ``sigma`` scales L (``L -> sigma*L``, E_corr scales as sigma**4).  The
+  "scaled twin" picks sigma so that |E_corr| is about 0.05*o Eh, where an
+  absolute micro-Hartree tolerance is meaningful.
+
+Generation order is fixed so a seed reproduces bit-identical arrays.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class SpinOrbitals:
+    C: np.ndarray      # (N, N) float64, C[mu, p]
+    eps: np.ndarray    # (N,) float64, ascending
+    nocc: int
+
+
+@dataclass
+class CDInputs:
+    N: int
+    M: int
+    L: np.ndarray                  # (M, N*N) float64, index mu*N+nu
+    alpha: SpinOrbitals
+    beta: SpinOrbitals | None = None
+    sigma: float = 1.0
+    seed: int = 0
+    H: np.ndarray | None = field(default=None, repr=False)  # core Hamiltonian (optional)
+
+    @property
+    def restricted(self) -> bool:
+        return self.beta is None
+
+
+def scale_factors(M: int) -> np.ndarray:
+    q = np.arange(M, dtype=np.float64)
+    return 10.0 ** (-6.0 * q / M)
+
+
+def _orbital_energies(rng: np.random.Generator, N: int, nocc: int) -> np.ndarray:
+    n_low = min(4, nocc)
+    occ = rng.uniform(-2.0, -0.3, size=nocc)
+    occ.sort()
+    occ[:n_low] = -20.0
+    vir = np.exp(rng.uniform(math.log(0.05), math.log(5.0), size=N - nocc))
+    vir.sort()
+    return np.concatenate([occ, vir])
+
+
+def _orthogonal(rng: np.random.Generator, N: int) -> np.ndarray:
+    q, r = np.linalg.qr(rng.standard_normal((N, N)))
+    # fix the sign convention so the factor is unique for a given matrix
+    q *= np.sign(np.diag(r))[None, :]
+    return np.ascontiguousarray(q)
+
+
+def make_vectors(rng: np.random.Generator, N: int, M: int, sigma: float = 1.0,
+                 dtype=np.float64, chunk: int = 64) -> np.ndarray:
+    """L as (M, N*N): L^Q = sigma * s_Q * (X + X^T)/2, X ~ N(0,1)."""
+    s = scale_factors(M) * sigma
+    L = np.empty((M, N * N), dtype=dtype)
+    for q0 in range(0, M, chunk):
+        q1 = min(M, q0 + chunk)
+        X = rng.standard_normal((q1 - q0, N, N))
+        G = 0.5 * (X + X.transpose(0, 2, 1))
+        G *= s[q0:q1, None, None]
+        L[q0:q1] = G.reshape(q1 - q0, N * N)
+    return L
+
+
+def make_inputs(N: int, nocc: int, M: int, seed: int = 0, sigma: float = 1.0,
+                nocc_beta: int | None = None, dtype=np.float64) -> CDInputs:
+    """Restricted inputs when ``nocc_beta`` is None, else separate alpha/beta
+    orbitals (distinct random orthogonal C_alpha, C_beta) sharing L."""
+    rng = np.random.default_rng(seed)
+    L = make_vectors(rng, N, M, sigma, dtype=dtype)
+    Ca = _orthogonal(rng, N)
+    ea = _orbital_energies(rng, N, nocc)
+    alpha = SpinOrbitals(Ca, ea, nocc)
+    beta = None
+    if nocc_beta is not None:
+        Cb = _orthogonal(rng, N)
+        eb = _orbital_energies(rng, N, nocc_beta)
+        beta = SpinOrbitals(Cb, eb, nocc_beta)
+    return CDInputs(N=N, M=M, L=L, alpha=alpha, beta=beta, sigma=sigma, seed=seed)
+
+
+def mean_inverse_denominator(eps_occ_i, eps_vir_a, eps_occ_j, eps_vir_b,
+                             samples: int = 1 << 20, seed: int = 12345) -> float:
+    rng = np.random.default_rng(seed)
+    i = rng.integers(0, len(eps_occ_i), samples)
+    j = rng.integers(0, len(eps_occ_j), samples)
+    a = rng.integers(0, len(eps_vir_a), samples)
+    b = rng.integers(0, len(eps_vir_b), samples)
+    d = eps_occ_i[i] + eps_occ_j[j] - eps_vir_a[a] - eps_vir_b[b]
+    return float(np.mean(1.0 / d))
+
+
+def twin_sigma(N: int, nocc: int, M: int, eps: np.ndarray,
+               target_per_occ: float = 0.05) -> float:
+    """sigma for which the recipe's expected |E_corr| is about target*o Eh.
+
+    Model: B^Q_ia ~ N(0, s_Q^2/2) for an orthogonal C (the symmetrised
+    Gaussian has off-diagonal variance 1/2 and is rotation invariant), so
+    Var((ia|jb)) = sum_Q s_Q^4 / 4 and E ~ 2 o^2 v^2 Var <1/D>.
+    """
+    v = N - nocc
+    s4 = float(np.sum(scale_factors(M) ** 4))
+    var = s4 / 4.0
+    inv_d = abs(mean_inverse_denominator(eps[:nocc], eps[nocc:], eps[:nocc], eps[nocc:]))
+    e1 = 2.0 * nocc * nocc * v * v * var * inv_d
+    return (target_per_occ * nocc / e1) ** 0.25
+
+
+def default_core_hamiltonian(inp: CDInputs) -> np.ndarray:
+    """H such that the reference-density Fock operator of spin alpha is
+    C diag(eps) C^T (an orthonormal AO basis, S = I):
+    H = C_a diag(eps_a) C_a^T - J[P_a + P_b] + K[P_a], with the Cholesky J/K of
+    reference src/mp2/cholesky_omp2.cc:347-358."""
+    N = inp.N
+    a = inp.alpha
+    b = inp.beta if inp.beta is not None else inp.alpha
+    Pa = a.C[:, :a.nocc] @ a.C[:, :a.nocc].T
+    Pb = b.C[:, :b.nocc] @ b.C[:, :b.nocc].T
+    Ptot = Pa + Pb
+    L3 = inp.L.reshape(inp.M, N, N)
+    J = np.zeros((N, N))
+    K = np.zeros((N, N))
+    for q in range(inp.M):
+        Lq = L3[q].T  # Eigen column-major map of the vector
+        J += np.sum(Lq * Ptot) * Lq
+        K += Lq @ Pa @ Lq
+    F = (a.C * a.eps[None, :]) @ a.C.T
+    return F - J + K
