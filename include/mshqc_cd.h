@@ -1,0 +1,144 @@
+/*
+ * mshqc_cd.h -- C ABI of the B200 Cholesky-vector MP2 library
+ * (libmshqc_cuda.so).
+ *
+ * The library replaces the compute inside mshqc's CD-RMP2 / CD-UMP2 /
+ * CD-OMP2 classes.  Every function returns an int status (0 = ok, negative =
+ * error, see MSHQC_CD_ERR_*); the message of the last failure on the calling
+ * thread is available from mshqc_cd_last_error().  No function calls exit()
+ * or throws.  A context is single-threaded and stream-ordered: calls on one
+ * context must not overlap; results are complete when a call returns.
+ *
+ * Array conventions (the reference's own, so its data can be passed as-is):
+ *   L     AO Cholesky vectors, M vectors of N*N doubles, vector Q element
+ *         mu*N+nu (CholeskyERI::L_vectors_, reference
+ *         include/mshqc/integrals/cholesky_eri.h:67,81,89-91).  Packed layout:
+ *         N(N+1)/2 doubles per vector, the upper triangle mu<=nu row by row.
+ *   C     N*N MO coefficients, column-major (Eigen::MatrixXd, reference
+ *         SCFResult::C_alpha include/mshqc/scf.h:83); the first nocc columns
+ *         are occupied (leftCols(nocc)).
+ *   eps   N orbital energies (SCFResult::orbital_energies_alpha, scf.h:77).
+ *   B     MO vectors B^Q_ia, o*v*M doubles, element (i*v + a)*M + Q.
+ *   dC    N*N column-major, dE/dC[mu, p].
+ *   grad  v*o column-major orbital gradient g[a, i] = dE/dkappa_ai for
+ *         C -> C exp(-kappa), kappa_ai = -kappa_ia (rotation of reference
+ *         src/mp2/cholesky_omp2.cc:385-396), orbital energies held fixed.
+ */
+#ifndef MSHQC_CD_H
+#define MSHQC_CD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSHQC_CD_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define MSHQC_CD_API __attribute__((visibility("default")))
+#else
+#define MSHQC_CD_API
+#endif
+
+enum mshqc_cd_status {
+    MSHQC_CD_OK = 0,
+    MSHQC_CD_ERR_ARG = -1,         /* invalid argument or shape              */
+    MSHQC_CD_ERR_STATE = -2,       /* call order (e.g. energy before inputs) */
+    MSHQC_CD_ERR_CUDA = -3,        /* CUDA runtime / driver error            */
+    MSHQC_CD_ERR_ALLOC = -4,       /* device allocation failed               */
+    MSHQC_CD_ERR_NUMERIC = -5,     /* NaN / Inf in the inputs                */
+    MSHQC_CD_ERR_UNSUPPORTED = -6, /* no such device / not sm_100            */
+    MSHQC_CD_ERR_TIMEOUT = -7      /* a device-side bounded wait gave up     */
+};
+
+enum mshqc_cd_precision {
+    MSHQC_CD_FP64 = 0,   /* FP64 contractions (DMMA)                        */
+    MSHQC_CD_BF16X3 = 1  /* hi/lo BF16 split, 3 products, FP32 accumulate on
+                            the tensor cores; FP64 denominators and energies */
+};
+
+enum mshqc_cd_kind {
+    MSHQC_CD_RESTRICTED = 0,   /* closed shell, one set of orbitals (RMP2) */
+    MSHQC_CD_UNRESTRICTED = 1  /* alpha and beta orbitals (UMP2 / OMP2)    */
+};
+
+enum mshqc_cd_layout { MSHQC_CD_LAYOUT_FULL = 0, MSHQC_CD_LAYOUT_PACKED = 1 };
+enum mshqc_cd_where { MSHQC_CD_HOST = 0, MSHQC_CD_DEVICE = 1 };
+enum mshqc_cd_spin { MSHQC_CD_ALPHA = 0, MSHQC_CD_BETA = 1 };
+
+typedef struct mshqc_cd_ctx mshqc_cd_ctx;
+
+/* Energy components (Eh).  Restricted: total = e_corr of CholeskyRMP2;
+ * ss_aa = ss_bb and os are its same-/opposite-spin parts.  Unrestricted:
+ * the CholeskyUMP2Result fields e_corr_ss_aa/_ss_bb/_os/_total
+ * (reference include/mshqc/cholesky_ump2.h:51-68).  Stage times in ms,
+ * measured with CUDA events on the context stream. */
+typedef struct {
+    double ss_aa, ss_bb, os, total;
+    double ms_transform, ms_energy, ms_total;
+} mshqc_cd_energy;
+
+/* --- context ---------------------------------------------------------- */
+/* Replaces: nothing in the reference (it keeps no device state); owns the
+ * device, the stream and the grow-only workspaces. */
+MSHQC_CD_API int mshqc_cd_ctx_create(int device, mshqc_cd_ctx** out);
+MSHQC_CD_API int mshqc_cd_ctx_destroy(mshqc_cd_ctx* ctx);
+MSHQC_CD_API const char* mshqc_cd_last_error(void);
+MSHQC_CD_API int mshqc_cd_abi_version(void);
+/* Run on a caller stream (cudaStream_t) instead of the context's own. */
+MSHQC_CD_API int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream);
+/* Bytes of device memory the context holds. */
+MSHQC_CD_API int mshqc_cd_device_bytes(mshqc_cd_ctx* ctx, int64_t* bytes);
+/* Number of kernels this context has launched so far. */
+MSHQC_CD_API int mshqc_cd_launch_count(mshqc_cd_ctx* ctx, int64_t* count);
+
+/* --- inputs ----------------------------------------------------------- */
+/* AO Cholesky vectors.  Replaces the CholeskyERI container read by the
+ * transforms (reference src/mp2/cholesky_rmp2.cc:69-71,
+ * src/mp2/cholesky_ump2.cc:250, src/mp2/cholesky_omp2.cc:77). */
+MSHQC_CD_API int mshqc_cd_set_vectors(mshqc_cd_ctx* ctx, const double* L, int64_t nbf,
+                         int64_t nvec, int layout, int where);
+/* Orbitals of one spin.  Replaces the SCFResult fields C_alpha/C_beta,
+ * orbital_energies_alpha/beta, n_occ_alpha/beta read by the MP2 classes
+ * (reference src/mp2/cholesky_rmp2.cc:27-29,77-78,106;
+ * src/mp2/cholesky_ump2.cc:41-44,255-258). */
+MSHQC_CD_API int mshqc_cd_set_orbitals(mshqc_cd_ctx* ctx, int spin, const double* C,
+                          const double* eps, int64_t nocc, int where);
+
+/* --- forward ---------------------------------------------------------- */
+/* AO->MO half transform B^Q_ia = sum C_mu,i L^Q_mu,nu C_nu,a of one spin.
+ * Replaces CholeskyRMP2::transform_vectors (src/mp2/cholesky_rmp2.cc:68-93),
+ * CholeskyUMP2::transform_cholesky_vectors (src/mp2/cholesky_ump2.cc:244-293)
+ * and CholeskyOMP2::transform_vectors (src/mp2/cholesky_omp2.cc:71-92).
+ * B_out (o*v*M, see header) may be NULL to keep the result on the device
+ * only. */
+MSHQC_CD_API int mshqc_cd_transform(mshqc_cd_ctx* ctx, int spin, int precision,
+                       double* B_out, int where);
+/* MP2 correlation energy.  Replaces the pair loop of CholeskyRMP2::compute
+ * (src/mp2/cholesky_rmp2.cc:118-153) for kind RESTRICTED and
+ * CholeskyUMP2::compute_ss_alpha/compute_ss_beta/compute_os
+ * (src/mp2/cholesky_ump2.cc:299-465) for kind UNRESTRICTED; runs the
+ * transforms first when the orbitals changed. */
+MSHQC_CD_API int mshqc_cd_mp2_energy(mshqc_cd_ctx* ctx, int kind, int precision,
+                        mshqc_cd_energy* out);
+/* Pair energies of the last mp2_energy call: restricted o*o (e_ij, all
+ * ordered pairs, symmetric); unrestricted block 0 = aa (oa*oa), 1 = bb,
+ * 2 = ab (oa*ob).  Row-major [i][j]. */
+MSHQC_CD_API int mshqc_cd_pair_energies(mshqc_cd_ctx* ctx, int block, double* out, int where);
+
+/* --- backward (exact differentiation; no reference counterpart) ------- */
+/* Energy and its exact derivatives with respect to the orbitals and the
+ * orbital energies.  dC_a/dC_b: N*N column-major; deps_a/deps_b: N; any
+ * output may be NULL.  For RESTRICTED only the _a outputs are written and
+ * they are the derivatives of the closed-shell energy with respect to the
+ * one shared C and eps.  e_out may be NULL. */
+MSHQC_CD_API int mshqc_cd_mp2_gradient(mshqc_cd_ctx* ctx, int kind, int precision,
+                          mshqc_cd_energy* e_out, double* dC_a, double* dC_b,
+                          double* deps_a, double* deps_b, int where);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MSHQC_CD_H */

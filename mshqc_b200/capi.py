@@ -1,0 +1,241 @@
+"""ctypes binding of the C ABI in include/mshqc_cd.h (libmshqc_cuda.so).
+
+This is the only way the Python side reaches the GPU: there is no CPU
+fallback.  If the library is missing, importing this module still works (so
+that CPU-only tooling can inspect it) but creating a Context raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmshqc_cuda.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mshqc_cd.h")
+
+OK = 0
+ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_NUMERIC, ERR_UNSUPPORTED, ERR_TIMEOUT = (
+    -1, -2, -3, -4, -5, -6, -7)
+FP64, BF16X3 = 0, 1
+RESTRICTED, UNRESTRICTED = 0, 1
+LAYOUT_FULL, LAYOUT_PACKED = 0, 1
+HOST, DEVICE = 0, 1
+ALPHA, BETA = 0, 1
+
+PRECISIONS = {"fp64": FP64, "bf16x3": BF16X3}
+
+
+class CDError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Energy(ctypes.Structure):
+    _fields_ = [("ss_aa", ctypes.c_double), ("ss_bb", ctypes.c_double),
+                ("os", ctypes.c_double), ("total", ctypes.c_double),
+                ("ms_transform", ctypes.c_double), ("ms_energy", ctypes.c_double),
+                ("ms_total", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int
+_i64 = ctypes.c_int64
+# name -> (restype, argtypes); the set of exported entry points
+SIGNATURES = {
+    "mshqc_cd_ctx_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
+    "mshqc_cd_ctx_destroy": (_i32, [_vp]),
+    "mshqc_cd_last_error": (ctypes.c_char_p, []),
+    "mshqc_cd_abi_version": (_i32, []),
+    "mshqc_cd_set_stream": (_i32, [_vp, _vp]),
+    "mshqc_cd_device_bytes": (_i32, [_vp, ctypes.POINTER(_i64)]),
+    "mshqc_cd_launch_count": (_i32, [_vp, ctypes.POINTER(_i64)]),
+    "mshqc_cd_set_vectors": (_i32, [_vp, _vp, _i64, _i64, _i32, _i32]),
+    "mshqc_cd_set_orbitals": (_i32, [_vp, _i32, _vp, _vp, _i64, _i32]),
+    "mshqc_cd_transform": (_i32, [_vp, _i32, _i32, _vp, _i32]),
+    "mshqc_cd_mp2_energy": (_i32, [_vp, _i32, _i32, ctypes.POINTER(Energy)]),
+    "mshqc_cd_pair_energies": (_i32, [_vp, _i32, _vp, _i32]),
+    "mshqc_cd_mp2_gradient": (_i32, [_vp, _i32, _i32, ctypes.POINTER(Energy), _vp, _vp, _vp,
+                                     _vp, _i32]),
+}
+
+_lib = None
+
+
+def library_available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def load_library():
+    """Load libmshqc_cuda.so (fails loudly if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not library_available():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m mshqc_b200.build` "
+                "(there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise CDError(rc, load_library().mshqc_cd_last_error().decode())
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _host_f64(x, order="C"):
+    a = np.asarray(x, dtype=np.float64)
+    return np.asfortranarray(a) if order == "F" else np.ascontiguousarray(a)
+
+
+def _ptr(a):
+    if _is_torch_cuda(a):
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class Gradient:
+    energy: dict
+    dC_a: np.ndarray | None
+    dC_b: np.ndarray | None
+    deps_a: np.ndarray | None
+    deps_b: np.ndarray | None
+
+
+class Context:
+    """One device context (stream + workspaces) of libmshqc_cuda."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self._lib.mshqc_cd_ctx_create(device, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+        self.nbf = 0
+        self.nvec = 0
+        self.nocc = [0, 0]
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.mshqc_cd_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_handle: int | None):
+        _check(self._lib.mshqc_cd_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64(0)
+        _check(self._lib.mshqc_cd_device_bytes(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def launch_count(self) -> int:
+        c = ctypes.c_int64(0)
+        _check(self._lib.mshqc_cd_launch_count(self._h, ctypes.byref(c)))
+        return int(c.value)
+
+    # -- inputs -----------------------------------------------------------
+    def set_vectors(self, L, nbf: int | None = None, layout: str = "full"):
+        """L: (M, N*N) host array or CUDA tensor (or packed (M, N(N+1)/2))."""
+        lay = LAYOUT_PACKED if layout == "packed" else LAYOUT_FULL
+        if _is_torch_cuda(L):
+            import torch
+            L = L.to(torch.float64).contiguous()
+            where = DEVICE
+        else:
+            L = _host_f64(L)
+            where = HOST
+        M = L.shape[0]
+        if nbf is None:
+            per = L.shape[1] if L.ndim == 2 else int(np.prod(L.shape[1:]))
+            nbf = int(round(per ** 0.5)) if lay == LAYOUT_FULL else int((np.sqrt(8 * per + 1) - 1) / 2)
+        _check(self._lib.mshqc_cd_set_vectors(self._h, _ptr(L), int(nbf), int(M), lay, where))
+        self.nbf, self.nvec = int(nbf), int(M)
+        return self
+
+    def set_orbitals(self, spin: int, C, eps, nocc: int):
+        """C[mu, p] (N x N), eps (N,), first nocc columns occupied."""
+        if _is_torch_cuda(C):
+            import torch
+            Cc = C.to(torch.float64).t().contiguous()     # column-major bytes
+            ec = eps.to(torch.float64).contiguous()
+            where = DEVICE
+        else:
+            Cc = _host_f64(C, "F")
+            ec = _host_f64(eps)
+            where = HOST
+        _check(self._lib.mshqc_cd_set_orbitals(self._h, spin, _ptr(Cc), _ptr(ec), int(nocc), where))
+        self.nocc[spin] = int(nocc)
+        return self
+
+    # -- forward ----------------------------------------------------------
+    def transform(self, spin: int = ALPHA, precision: int = FP64) -> np.ndarray:
+        o = self.nocc[spin]
+        v = self.nbf - o
+        out = np.empty((o, v, self.nvec), dtype=np.float64)
+        _check(self._lib.mshqc_cd_transform(self._h, spin, precision, _ptr(out), HOST))
+        return out
+
+    def mp2_energy(self, kind: int = RESTRICTED, precision: int = FP64) -> dict:
+        e = Energy()
+        _check(self._lib.mshqc_cd_mp2_energy(self._h, kind, precision, ctypes.byref(e)))
+        return e.as_dict()
+
+    def pair_energies(self, block: int = 0) -> np.ndarray:
+        oa, ob = self.nocc
+        rows, cols = {0: (oa, oa), 1: (ob, ob), 2: (oa, ob)}[block]
+        out = np.empty((rows, cols), dtype=np.float64)
+        _check(self._lib.mshqc_cd_pair_energies(self._h, block, _ptr(out), HOST))
+        return out
+
+    # -- backward ---------------------------------------------------------
+    def mp2_gradient(self, kind: int = RESTRICTED, precision: int = FP64) -> Gradient:
+        N = self.nbf
+        e = Energy()
+        dCa = np.zeros((N, N), dtype=np.float64, order="F")
+        dea = np.zeros(N, dtype=np.float64)
+        if kind == UNRESTRICTED:
+            dCb = np.zeros((N, N), dtype=np.float64, order="F")
+            deb = np.zeros(N, dtype=np.float64)
+        else:
+            dCb = deb = None
+        _check(self._lib.mshqc_cd_mp2_gradient(
+            self._h, kind, precision, ctypes.byref(e), _ptr(dCa),
+            _ptr(dCb) if dCb is not None else None, _ptr(dea),
+            _ptr(deb) if deb is not None else None, HOST))
+        return Gradient(e.as_dict(), dCa, dCb, dea, deb)
+
+
+def exported_symbols_from_header(path: str = HEADER) -> list[str]:
+    """Function names declared with MSHQC_CD_API in include/mshqc_cd.h."""
+    import re
+    txt = open(path).read()
+    return sorted(set(re.findall(r"MSHQC_CD_API\s+[\w\s\*]*?\b(mshqc_cd_\w+)\s*\(", txt)))

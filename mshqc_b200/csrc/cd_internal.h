@@ -1,0 +1,131 @@
+// Internal state of a libmshqc_cuda context (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mshqc_cd.h"
+
+namespace mshqc_cd {
+
+// Grow-only device allocation: a context allocates on the first call at a
+// given size and reuses the memory afterwards.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t nbytes, bool zero, cudaStream_t st);
+    void release();
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct DeviceGuard {
+    int prev = 0, target = 0;
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+};
+
+struct SpinState {
+    DevBuf C, eps;          // N*N column-major, N
+    int64_t nocc = 0;
+    bool set = false;
+    // FP64 MO vectors [i][a][Q] (a padded to vp, Q to Mp)
+    DevBuf B64;
+    int64_t vp = 0;
+    bool B64_valid = false;
+    // BF16 hi/lo split of the MO vectors for the tensor-core path
+    DevBuf Bhi, Blo;
+    int64_t vp16 = 0, Mp16 = 0;
+    bool B16_valid = false;
+    void invalidate() {
+        B64_valid = false;
+        B16_valid = false;
+    }
+};
+
+}  // namespace mshqc_cd
+
+struct mshqc_cd_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    void* bounce[2] = {nullptr, nullptr};
+    cudaEvent_t bounce_ev[2] = {nullptr, nullptr};
+
+    int64_t N = 0, M = 0, Mp = 0;
+    bool L_set = false;
+    int64_t launches = 0;           // kernels launched by this context
+    mshqc_cd::DevBuf L;             // [Q][N*N] FP64
+    mshqc_cd::SpinState spin[2];
+
+    // workspaces
+    mshqc_cd::DevBuf Y;             // half-transformed vectors
+    mshqc_cd::DevBuf scratch;       // uploads / unpacking
+    mshqc_cd::DevBuf tables;        // pair and block tables
+    mshqc_cd::DevBuf partial;       // per-unit energies
+    mshqc_cd::DevBuf pair_sum;      // per-pair energies
+    mshqc_cd::DevBuf totals;        // scalar results
+    mshqc_cd::DevBuf flag;          // error / NaN flags
+    mshqc_cd::DevBuf amp;           // backward: staged amplitudes
+    mshqc_cd::DevBuf gam[2];        // backward: Gamma per spin
+    mshqc_cd::DevBuf BT;            // backward: transposed MO vectors
+    mshqc_cd::DevBuf W;             // backward: C_vir-contracted Gamma
+    mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
+
+    std::vector<double> pair_energy[3];  // host copies, row-major [i][j]
+
+    void invalidate_all() {
+        spin[0].invalidate();
+        spin[1].invalidate();
+        for (auto& p : pair_energy) p.clear();
+    }
+    size_t held_bytes() const {
+        size_t b = L.bytes + Y.bytes + scratch.bytes + tables.bytes + partial.bytes +
+                   pair_sum.bytes + totals.bytes + flag.bytes + amp.bytes + BT.bytes + W.bytes;
+        for (const auto& s : spin) b += s.C.bytes + s.eps.bytes + s.B64.bytes + s.Bhi.bytes + s.Blo.bytes;
+        for (const auto& g : gam) b += g.bytes;
+        for (const auto& g : grad) b += g.bytes;
+        return b;
+    }
+    void release_all() {
+        L.release();
+        Y.release();
+        scratch.release();
+        tables.release();
+        partial.release();
+        pair_sum.release();
+        totals.release();
+        flag.release();
+        amp.release();
+        BT.release();
+        W.release();
+        for (auto& s : spin) {
+            s.C.release();
+            s.eps.release();
+            s.B64.release();
+            s.Bhi.release();
+            s.Blo.release();
+        }
+        for (auto& g : gam) g.release();
+        for (auto& g : grad) g.release();
+    }
+};
+
+namespace mshqc_cd {
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+int upload(mshqc_cd_ctx* ctx, void* dst, const void* src, size_t nbytes);
+int download(mshqc_cd_ctx* ctx, void* dst, const void* src, size_t nbytes, int where);
+int check_finite_device(mshqc_cd_ctx* ctx, const double* x, int64_t n, const char* what);
+
+// implemented in cd_mp2.cu
+int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision);
+int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out);
+int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out,
+                 double* dC_a, double* dC_b, double* deps_a, double* deps_b, int where);
+}  // namespace mshqc_cd

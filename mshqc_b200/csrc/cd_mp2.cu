@@ -1,0 +1,257 @@
+// Orchestration of the Cholesky-MP2 kernels: half transforms, pair energies,
+// reductions.  Called from the C ABI (cd_abi.cu) with the device selected.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cd_common.cuh"
+#include "cd_internal.h"
+#include "gemm_f64.cuh"
+#include "pair_energy_f64.cuh"
+
+namespace mshqc_cd {
+
+#define CD_CUDA(call)                                                     \
+    do {                                                                  \
+        cudaError_t _e = (call);                                          \
+        if (_e != cudaSuccess) return cuda_error(_e, #call);              \
+    } while (0)
+#define CD_ALLOC(buf, nbytes, zero)                                                        \
+    do {                                                                                   \
+        cudaError_t _e = (buf).reserve((nbytes), (zero), ctx->stream);                     \
+        if (_e == cudaErrorMemoryAllocation)                                               \
+            return set_error(MSHQC_CD_ERR_ALLOC, "device allocation of " +                 \
+                                                     std::to_string((size_t)(nbytes)) +    \
+                                                     " bytes failed");                     \
+        if (_e != cudaSuccess) return cuda_error(_e, "workspace");                         \
+    } while (0)
+#define CD_RC(x)             \
+    do {                     \
+        int _rc = (x);       \
+        if (_rc) return _rc; \
+    } while (0)
+
+namespace {
+
+int require_inputs(mshqc_cd_ctx* ctx, int spin) {
+    if (!ctx->L_set) return set_error(MSHQC_CD_ERR_STATE, "Cholesky vectors not set");
+    if (!ctx->spin[spin].set)
+        return set_error(MSHQC_CD_ERR_STATE,
+                         spin == 0 ? "alpha orbitals not set" : "beta orbitals not set");
+    return MSHQC_CD_OK;
+}
+
+// FP64 half transform of one spin into the padded [i][a][Q] layout.
+int transform_f64(mshqc_cd_ctx* ctx, int spin) {
+    SpinState& s = ctx->spin[spin];
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o;
+    const int64_t vp = round_up(v, 64);
+    CD_ALLOC(ctx->Y, sizeof(double) * (size_t)o * M * N, false);
+    CD_ALLOC(s.B64, sizeof(double) * (size_t)o * vp * Mp, true);
+    s.vp = vp;
+    const double* C = s.C.as<double>();
+    // Y[i][(Q,nu)] = sum_mu C[mu,i] L[Q][nu*N + mu]
+    GemmF64Args g1{};
+    g1.M = (int)o;
+    g1.N = (int)(M * N);
+    g1.K = (int)N;
+    g1.batch = 1;
+    g1.A = C;  g1.lda = N;  g1.sA = 0;
+    g1.B = ctx->L.as<double>();  g1.ldb = N;  g1.sB = 0;
+    g1.C = ctx->Y.as<double>();  g1.ldc = M * N;  g1.sC = 0;
+    g1.alpha = 1.0;  g1.beta = 0.0;
+    CD_CUDA(gemm_f64(g1, true, true, ctx->stream));
+    ctx->launches++;
+    // B[i][a][Q] = sum_nu C[nu, o+a] Y[i][Q][nu]
+    GemmF64Args g2{};
+    g2.M = (int)v;
+    g2.N = (int)M;
+    g2.K = (int)N;
+    g2.batch = (int)o;
+    g2.A = C + o * N;  g2.lda = N;  g2.sA = 0;
+    g2.B = ctx->Y.as<double>();  g2.ldb = N;  g2.sB = M * N;
+    g2.C = s.B64.as<double>();  g2.ldc = Mp;  g2.sC = vp * Mp;
+    g2.alpha = 1.0;  g2.beta = 0.0;
+    CD_CUDA(gemm_f64(g2, true, true, ctx->stream));
+    ctx->launches++;
+    s.B64_valid = true;
+    return MSHQC_CD_OK;
+}
+
+struct UnitTables {
+    std::vector<int2> pairs, blocks;
+};
+
+UnitTables make_tables(int mode, int ox, int oy, int nbx, int nby) {
+    UnitTables t;
+    if (mode == PAIR_OPPOSITE_SPIN) {
+        for (int i = 0; i < ox; ++i)
+            for (int j = 0; j < oy; ++j) t.pairs.push_back(make_int2(i, j));
+        for (int x = 0; x < nbx; ++x)
+            for (int y = 0; y < nby; y += 2) t.blocks.push_back(make_int2(x, y));
+    } else {
+        for (int i = 0; i < ox; ++i)
+            for (int j = (mode == PAIR_RESTRICTED ? i : i + 1); j < ox; ++j)
+                t.pairs.push_back(make_int2(i, j));
+        for (int x = 0; x < nbx; ++x)
+            for (int y = x; y < nbx; ++y) t.blocks.push_back(make_int2(x, y));
+    }
+    return t;
+}
+
+// One FP64 pair-energy pass.  Returns the total in *total and fills the
+// ordered pair-energy matrix (row-major ox*oy) in pair_mat.
+int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
+                  std::vector<double>& pair_mat, double* total_os = nullptr) {
+    const SpinState& X = ctx->spin[sx];
+    const SpinState& Y = ctx->spin[sy];
+    const int ox = (int)X.nocc, oy = (int)Y.nocc;
+    const int vx = (int)(ctx->N - ox), vy = (int)(ctx->N - oy);
+    const int nbx = (int)(X.vp / 64), nby = (int)(Y.vp / 64);
+    UnitTables t = make_tables(mode, ox, oy, nbx, nby);
+    const int npairs = (int)t.pairs.size(), nblocks = (int)t.blocks.size();
+    pair_mat.assign((size_t)ox * oy, 0.0);
+    *total = 0.0;
+    if (npairs == 0 || nblocks == 0) return MSHQC_CD_OK;
+
+    const size_t tbytes = sizeof(int2) * (t.pairs.size() + t.blocks.size());
+    CD_ALLOC(ctx->tables, tbytes, false);
+    int2* dpairs = ctx->tables.as<int2>();
+    int2* dblocks = dpairs + npairs;
+    CD_CUDA(cudaMemcpyAsync(dpairs, t.pairs.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    CD_CUDA(cudaMemcpyAsync(dblocks, t.blocks.data(), sizeof(int2) * nblocks,
+                            cudaMemcpyHostToDevice, ctx->stream));
+    const int64_t units = (int64_t)npairs * nblocks;
+    CD_ALLOC(ctx->partial, sizeof(double) * units * 2, false);
+    CD_ALLOC(ctx->pair_sum, sizeof(double) * npairs * 2, false);
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+
+    PairF64Args a{};
+    a.X = X.B64.as<double>();
+    a.Y = Y.B64.as<double>();
+    a.vx = vx;  a.vy = vy;
+    a.vpx = (int)X.vp;  a.vpy = (int)Y.vp;
+    a.Mp = (int)ctx->Mp;
+    a.eox = X.eps.as<double>();  a.evx = a.eox + ox;
+    a.eoy = Y.eps.as<double>();  a.evy = a.eoy + oy;
+    a.pairs = dpairs;
+    a.blocks = dblocks;
+    a.nblocks = nblocks;
+    a.partial = ctx->partial.as<double>();
+    a.partial2 = ctx->partial.as<double>() + units;
+    const size_t smem = pair_f64_detail::SMEM_BYTES;
+    if (mode == PAIR_RESTRICTED) {
+        CD_CUDA(cudaFuncSetAttribute(pair_energy_f64_kernel<PAIR_RESTRICTED>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        pair_energy_f64_kernel<PAIR_RESTRICTED><<<(unsigned)units, 256, smem, ctx->stream>>>(a);
+    } else if (mode == PAIR_SAME_SPIN) {
+        CD_CUDA(cudaFuncSetAttribute(pair_energy_f64_kernel<PAIR_SAME_SPIN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        pair_energy_f64_kernel<PAIR_SAME_SPIN><<<(unsigned)units, 256, smem, ctx->stream>>>(a);
+    } else {
+        CD_CUDA(cudaFuncSetAttribute(pair_energy_f64_kernel<PAIR_OPPOSITE_SPIN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        pair_energy_f64_kernel<PAIR_OPPOSITE_SPIN><<<(unsigned)units, 256, smem, ctx->stream>>>(a);
+    }
+    CD_CUDA(cudaGetLastError());
+    ctx->launches += 3;   // pair kernel + two reductions
+    reduce_pairs_kernel<<<(unsigned)cdiv(npairs, 128), 128, 0, ctx->stream>>>(
+        ctx->partial.as<double>(), npairs, nblocks, ctx->pair_sum.as<double>());
+    CD_CUDA(cudaGetLastError());
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->pair_sum.as<double>(), npairs,
+                                                   ctx->totals.as<double>());
+    CD_CUDA(cudaGetLastError());
+    if (mode == PAIR_RESTRICTED && total_os) {
+        ctx->launches += 2;
+        reduce_pairs_kernel<<<(unsigned)cdiv(npairs, 128), 128, 0, ctx->stream>>>(
+            ctx->partial.as<double>() + units, npairs, nblocks, ctx->pair_sum.as<double>() + npairs);
+        CD_CUDA(cudaGetLastError());
+        reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->pair_sum.as<double>() + npairs, npairs,
+                                                       ctx->totals.as<double>() + 1);
+        CD_CUDA(cudaGetLastError());
+        CD_CUDA(cudaMemcpyAsync(total_os, ctx->totals.as<double>() + 1, sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    std::vector<double> ps(npairs);
+    CD_CUDA(cudaMemcpyAsync(ps.data(), ctx->pair_sum.p, sizeof(double) * npairs,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaMemcpyAsync(total, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int p = 0; p < npairs; ++p) {
+        const int i = t.pairs[p].x, j = t.pairs[p].y;
+        if (mode == PAIR_OPPOSITE_SPIN) {
+            pair_mat[(size_t)i * oy + j] = ps[p];
+        } else if (i == j) {
+            pair_mat[(size_t)i * ox + j] = ps[p];
+        } else {
+            pair_mat[(size_t)i * ox + j] = 0.5 * ps[p];
+            pair_mat[(size_t)j * ox + i] = 0.5 * ps[p];
+        }
+    }
+    return MSHQC_CD_OK;
+}
+
+}  // namespace
+
+int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
+    CD_RC(require_inputs(ctx, spin));
+    SpinState& s = ctx->spin[spin];
+    if (precision == MSHQC_CD_FP64 || precision == MSHQC_CD_BF16X3) {
+        if (!s.B64_valid) CD_RC(transform_f64(ctx, spin));
+        return MSHQC_CD_OK;
+    }
+    return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
+}
+
+int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out) {
+    std::memset(out, 0, sizeof(*out));
+    if (precision != MSHQC_CD_FP64)
+        return set_error(MSHQC_CD_ERR_UNSUPPORTED, "BF16X3 energy path not built yet");
+    CD_RC(require_inputs(ctx, 0));
+    if (kind == MSHQC_CD_UNRESTRICTED) CD_RC(require_inputs(ctx, 1));
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    CD_CUDA(cudaEventRecord(e0, ctx->stream));
+    CD_RC(ensure_transform(ctx, 0, precision));
+    if (kind == MSHQC_CD_UNRESTRICTED) CD_RC(ensure_transform(ctx, 1, precision));
+    CD_CUDA(cudaEventRecord(e1, ctx->stream));
+    for (auto& p : ctx->pair_energy) p.clear();
+    if (kind == MSHQC_CD_RESTRICTED) {
+        double e_os = 0.0, e_tot = 0.0;
+        CD_RC(pair_pass_f64(ctx, PAIR_RESTRICTED, 0, 0, &e_tot, ctx->pair_energy[0], &e_os));
+        out->total = e_tot;
+        out->os = e_os;
+        out->ss_aa = out->ss_bb = 0.5 * (e_tot - e_os);
+    } else {
+        double ss_a = 0, ss_b = 0, os = 0;
+        CD_RC(pair_pass_f64(ctx, PAIR_SAME_SPIN, 0, 0, &ss_a, ctx->pair_energy[0]));
+        CD_RC(pair_pass_f64(ctx, PAIR_SAME_SPIN, 1, 1, &ss_b, ctx->pair_energy[1]));
+        CD_RC(pair_pass_f64(ctx, PAIR_OPPOSITE_SPIN, 0, 1, &os, ctx->pair_energy[2]));
+        out->ss_aa = ss_a;
+        out->ss_bb = ss_b;
+        out->os = os;
+        out->total = ss_a + ss_b + os;
+    }
+    CD_CUDA(cudaEventRecord(e2, ctx->stream));
+    CD_CUDA(cudaEventSynchronize(e2));
+    float t01 = 0, t12 = 0;
+    CD_CUDA(cudaEventElapsedTime(&t01, e0, e1));
+    CD_CUDA(cudaEventElapsedTime(&t12, e1, e2));
+    out->ms_transform = t01;
+    out->ms_energy = t12;
+    out->ms_total = t01 + t12;
+    return MSHQC_CD_OK;
+}
+
+int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out, double* dC_a,
+                 double* dC_b, double* deps_a, double* deps_b, int where) {
+    (void)ctx; (void)kind; (void)precision; (void)e_out; (void)dC_a; (void)dC_b;
+    (void)deps_a; (void)deps_b; (void)where;
+    return set_error(MSHQC_CD_ERR_UNSUPPORTED, "gradient path not built yet");
+}
+
+}  // namespace mshqc_cd
