@@ -11,6 +11,8 @@
 #include "cd_internal.h"
 #include "gemm_f64.cuh"
 #include "pair_energy_f64.cuh"
+#include "pair_energy_tc.cuh"
+#include "split_bf16.cuh"
 
 namespace mshqc_cd {
 
@@ -102,6 +104,49 @@ UnitTables make_tables(int mode, int ox, int oy, int nbx, int nby) {
     return t;
 }
 
+// Deterministic reductions of per-unit partials into pair energies and totals,
+// and the host copy of the ordered pair-energy matrix.
+int reduce_and_collect(mshqc_cd_ctx* ctx, int mode, const UnitTables& t, int64_t units, int npairs,
+                       int nblocks, int ox, int oy, double* total, std::vector<double>& pair_mat,
+                       double* total_os) {
+    ctx->launches += 2;
+    reduce_pairs_kernel<<<(unsigned)cdiv(npairs, 128), 128, 0, ctx->stream>>>(
+        ctx->partial.as<double>(), npairs, nblocks, ctx->pair_sum.as<double>());
+    CD_CUDA(cudaGetLastError());
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->pair_sum.as<double>(), npairs,
+                                                   ctx->totals.as<double>());
+    CD_CUDA(cudaGetLastError());
+    if (mode == PAIR_RESTRICTED && total_os) {
+        ctx->launches += 2;
+        reduce_pairs_kernel<<<(unsigned)cdiv(npairs, 128), 128, 0, ctx->stream>>>(
+            ctx->partial.as<double>() + units, npairs, nblocks, ctx->pair_sum.as<double>() + npairs);
+        CD_CUDA(cudaGetLastError());
+        reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->pair_sum.as<double>() + npairs, npairs,
+                                                       ctx->totals.as<double>() + 1);
+        CD_CUDA(cudaGetLastError());
+        CD_CUDA(cudaMemcpyAsync(total_os, ctx->totals.as<double>() + 1, sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    std::vector<double> ps(npairs);
+    CD_CUDA(cudaMemcpyAsync(ps.data(), ctx->pair_sum.p, sizeof(double) * npairs,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaMemcpyAsync(total, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int p = 0; p < npairs; ++p) {
+        const int i = t.pairs[p].x, j = t.pairs[p].y;
+        if (mode == PAIR_OPPOSITE_SPIN) {
+            pair_mat[(size_t)i * oy + j] = ps[p];
+        } else if (i == j) {
+            pair_mat[(size_t)i * ox + j] = ps[p];
+        } else {
+            pair_mat[(size_t)i * ox + j] = 0.5 * ps[p];
+            pair_mat[(size_t)j * ox + i] = 0.5 * ps[p];
+        }
+    }
+    return MSHQC_CD_OK;
+}
+
 // One FP64 pair-energy pass.  Returns the total in *total and fills the
 // ordered pair-energy matrix (row-major ox*oy) in pair_mat.
 int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
@@ -158,41 +203,124 @@ int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
         pair_energy_f64_kernel<PAIR_OPPOSITE_SPIN><<<(unsigned)units, 256, smem, ctx->stream>>>(a);
     }
     CD_CUDA(cudaGetLastError());
-    ctx->launches += 3;   // pair kernel + two reductions
-    reduce_pairs_kernel<<<(unsigned)cdiv(npairs, 128), 128, 0, ctx->stream>>>(
-        ctx->partial.as<double>(), npairs, nblocks, ctx->pair_sum.as<double>());
+    ctx->launches++;
+    CD_RC(reduce_and_collect(ctx, mode, t, units, npairs, nblocks, ox, oy, total, pair_mat, total_os));
+    return MSHQC_CD_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// BF16x3 tensor-core path
+// ---------------------------------------------------------------------------
+int64_t tc_rows(int64_t v) {
+    const int64_t nblk = cdiv(v, 128);
+    return 128 * std::max<int64_t>(nblk + 1, round_up(nblk, 4));
+}
+
+// hi/lo BF16 split of one spin's FP64 MO vectors into the blocked layout
+int split_bf16(mshqc_cd_ctx* ctx, int spin) {
+    SpinState& s = ctx->spin[spin];
+    const int64_t o = s.nocc, v = ctx->N - s.nocc, M = ctx->M, Mp = ctx->Mp;
+    const int64_t rows = tc_rows(v), nqc = Mp / 16;
+    const size_t n = (size_t)o * nqc * rows * 16;
+    CD_ALLOC(s.Bhi, n * sizeof(uint16_t), false);
+    CD_ALLOC(s.Blo, n * sizeof(uint16_t), false);
+    s.vp16 = rows;
+    s.Mp16 = Mp;
+    const int64_t threads = o * nqc * rows * 2;
+    const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
+    split_bf16_blocked_kernel<<<blocks, 256, 0, ctx->stream>>>(
+        s.B64.as<double>(), s.vp, Mp, (int)v, (int)M, o, nqc, rows, s.Bhi.as<uint16_t>(),
+        s.Blo.as<uint16_t>());
     CD_CUDA(cudaGetLastError());
-    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->pair_sum.as<double>(), npairs,
-                                                   ctx->totals.as<double>());
-    CD_CUDA(cudaGetLastError());
-    if (mode == PAIR_RESTRICTED && total_os) {
-        ctx->launches += 2;
-        reduce_pairs_kernel<<<(unsigned)cdiv(npairs, 128), 128, 0, ctx->stream>>>(
-            ctx->partial.as<double>() + units, npairs, nblocks, ctx->pair_sum.as<double>() + npairs);
-        CD_CUDA(cudaGetLastError());
-        reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->pair_sum.as<double>() + npairs, npairs,
-                                                       ctx->totals.as<double>() + 1);
-        CD_CUDA(cudaGetLastError());
-        CD_CUDA(cudaMemcpyAsync(total_os, ctx->totals.as<double>() + 1, sizeof(double),
-                                cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->launches++;
+    s.B16_valid = true;
+    return MSHQC_CD_OK;
+}
+
+UnitTables make_tables_tc(int mode, int ox, int oy, int nbx, int nby) {
+    UnitTables t;
+    if (mode == PAIR_OPPOSITE_SPIN) {
+        for (int i = 0; i < ox; ++i)
+            for (int j = 0; j < oy; ++j) t.pairs.push_back(make_int2(i, j));
+        for (int x = 0; x < nbx; ++x)
+            for (int y = 0; y < nby; y += 4) t.blocks.push_back(make_int2(x, y));
+    } else {
+        for (int i = 0; i < ox; ++i)
+            for (int j = (mode == PAIR_RESTRICTED ? i : i + 1); j < ox; ++j)
+                t.pairs.push_back(make_int2(i, j));
+        for (int x = 0; x < nbx; ++x)
+            for (int y = x; y < nbx; y += 2) t.blocks.push_back(make_int2(x, y));
     }
-    std::vector<double> ps(npairs);
-    CD_CUDA(cudaMemcpyAsync(ps.data(), ctx->pair_sum.p, sizeof(double) * npairs,
-                            cudaMemcpyDeviceToHost, ctx->stream));
-    CD_CUDA(cudaMemcpyAsync(total, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost,
+    return t;
+}
+
+template <int MODE>
+cudaError_t launch_tc(const PairTcArgs& a, int grid, cudaStream_t st) {
+    const size_t smem = pair_tc::SMEM_BYTES;
+    cudaError_t e = cudaFuncSetAttribute(pair_energy_tc_kernel<MODE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    pair_energy_tc_kernel<MODE><<<grid, pair_tc::THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
+                 std::vector<double>& pair_mat, double* total_os = nullptr) {
+    const SpinState& X = ctx->spin[sx];
+    const SpinState& Y = ctx->spin[sy];
+    const int ox = (int)X.nocc, oy = (int)Y.nocc;
+    const int vx = (int)(ctx->N - ox), vy = (int)(ctx->N - oy);
+    const int nbx = (int)cdiv(vx, 128), nby = (int)cdiv(vy, 128);
+    UnitTables t = make_tables_tc(mode, ox, oy, nbx, nby);
+    const int npairs = (int)t.pairs.size(), nblocks = (int)t.blocks.size();
+    pair_mat.assign((size_t)ox * oy, 0.0);
+    *total = 0.0;
+    if (total_os) *total_os = 0.0;
+    if (npairs == 0 || nblocks == 0) return MSHQC_CD_OK;
+    const size_t tbytes = sizeof(int2) * (t.pairs.size() + t.blocks.size());
+    CD_ALLOC(ctx->tables, tbytes, false);
+    int2* dpairs = ctx->tables.as<int2>();
+    int2* dblocks = dpairs + npairs;
+    CD_CUDA(cudaMemcpyAsync(dpairs, t.pairs.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice,
                             ctx->stream));
-    CD_CUDA(cudaStreamSynchronize(ctx->stream));
-    for (int p = 0; p < npairs; ++p) {
-        const int i = t.pairs[p].x, j = t.pairs[p].y;
-        if (mode == PAIR_OPPOSITE_SPIN) {
-            pair_mat[(size_t)i * oy + j] = ps[p];
-        } else if (i == j) {
-            pair_mat[(size_t)i * ox + j] = ps[p];
-        } else {
-            pair_mat[(size_t)i * ox + j] = 0.5 * ps[p];
-            pair_mat[(size_t)j * ox + i] = 0.5 * ps[p];
-        }
-    }
+    CD_CUDA(cudaMemcpyAsync(dblocks, t.blocks.data(), sizeof(int2) * nblocks,
+                            cudaMemcpyHostToDevice, ctx->stream));
+    const int64_t units = (int64_t)npairs * nblocks;
+    CD_ALLOC(ctx->partial, sizeof(double) * units * 2, false);
+    CD_ALLOC(ctx->pair_sum, sizeof(double) * npairs * 2, false);
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+    CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
+
+    PairTcArgs a{};
+    a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
+    a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
+    a.rows_x = (int)X.vp16;  a.rows_y = (int)Y.vp16;
+    a.nqc = (int)(ctx->Mp / 16);
+    a.vx = vx;  a.vy = vy;
+    a.eox = X.eps.as<double>();  a.evx = a.eox + ox;
+    a.eoy = Y.eps.as<double>();  a.evy = a.eoy + oy;
+    a.pairs = dpairs;  a.blocks = dblocks;  a.nblocks = nblocks;
+    a.units = units;
+    a.partial = ctx->partial.as<double>();
+    a.partial2 = ctx->partial.as<double>() + units;
+    a.err = ctx->flag.as<int>();
+    const int grid = (int)std::min<int64_t>(units, ctx->num_sms);
+    cudaError_t e;
+    if (mode == PAIR_RESTRICTED)
+        e = launch_tc<PAIR_RESTRICTED>(a, grid, ctx->stream);
+    else if (mode == PAIR_SAME_SPIN)
+        e = launch_tc<PAIR_SAME_SPIN>(a, grid, ctx->stream);
+    else
+        e = launch_tc<PAIR_OPPOSITE_SPIN>(a, grid, ctx->stream);
+    if (e != cudaSuccess) return cuda_error(e, "pair_energy_tc_kernel launch");
+    ctx->launches++;
+    int herr = 0;
+    CD_CUDA(cudaMemcpyAsync(&herr, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_RC(reduce_and_collect(ctx, mode, t, units, npairs, nblocks, ox, oy, total, pair_mat, total_os));
+    if (herr)
+        return set_error(MSHQC_CD_ERR_TIMEOUT,
+                         "tensor-core pair kernel gave up waiting (site " + std::to_string(herr) + ")");
     return MSHQC_CD_OK;
 }
 
@@ -201,17 +329,23 @@ int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
 int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
     CD_RC(require_inputs(ctx, spin));
     SpinState& s = ctx->spin[spin];
-    if (precision == MSHQC_CD_FP64 || precision == MSHQC_CD_BF16X3) {
-        if (!s.B64_valid) CD_RC(transform_f64(ctx, spin));
-        return MSHQC_CD_OK;
+    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_BF16X3)
+        return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
+    if (!s.B64_valid) {
+        CD_RC(transform_f64(ctx, spin));
+        s.B16_valid = false;
     }
-    return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
+    if (precision == MSHQC_CD_BF16X3 && !s.B16_valid) CD_RC(split_bf16(ctx, spin));
+    return MSHQC_CD_OK;
 }
 
 int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out) {
     std::memset(out, 0, sizeof(*out));
-    if (precision != MSHQC_CD_FP64)
-        return set_error(MSHQC_CD_ERR_UNSUPPORTED, "BF16X3 energy path not built yet");
+    auto pass = [&](int mode, int sx, int sy, double* tot, std::vector<double>& pm,
+                    double* tot_os) {
+        return precision == MSHQC_CD_BF16X3 ? pair_pass_tc(ctx, mode, sx, sy, tot, pm, tot_os)
+                                            : pair_pass_f64(ctx, mode, sx, sy, tot, pm, tot_os);
+    };
     CD_RC(require_inputs(ctx, 0));
     if (kind == MSHQC_CD_UNRESTRICTED) CD_RC(require_inputs(ctx, 1));
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
@@ -222,15 +356,15 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
     for (auto& p : ctx->pair_energy) p.clear();
     if (kind == MSHQC_CD_RESTRICTED) {
         double e_os = 0.0, e_tot = 0.0;
-        CD_RC(pair_pass_f64(ctx, PAIR_RESTRICTED, 0, 0, &e_tot, ctx->pair_energy[0], &e_os));
+        CD_RC(pass(PAIR_RESTRICTED, 0, 0, &e_tot, ctx->pair_energy[0], &e_os));
         out->total = e_tot;
         out->os = e_os;
         out->ss_aa = out->ss_bb = 0.5 * (e_tot - e_os);
     } else {
         double ss_a = 0, ss_b = 0, os = 0;
-        CD_RC(pair_pass_f64(ctx, PAIR_SAME_SPIN, 0, 0, &ss_a, ctx->pair_energy[0]));
-        CD_RC(pair_pass_f64(ctx, PAIR_SAME_SPIN, 1, 1, &ss_b, ctx->pair_energy[1]));
-        CD_RC(pair_pass_f64(ctx, PAIR_OPPOSITE_SPIN, 0, 1, &os, ctx->pair_energy[2]));
+        CD_RC(pass(PAIR_SAME_SPIN, 0, 0, &ss_a, ctx->pair_energy[0], nullptr));
+        CD_RC(pass(PAIR_SAME_SPIN, 1, 1, &ss_b, ctx->pair_energy[1], nullptr));
+        CD_RC(pass(PAIR_OPPOSITE_SPIN, 0, 1, &os, ctx->pair_energy[2], nullptr));
         out->ss_aa = ss_a;
         out->ss_bb = ss_b;
         out->os = os;

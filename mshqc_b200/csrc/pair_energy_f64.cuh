@@ -42,7 +42,7 @@ struct PairF64Args {
     const int2* blocks; // (row block, column block) per unit of a pair, 64-blocks
     int nblocks;
     double* partial;    // [npairs * nblocks]
-    double* partial2;   // RESTRICTED: opposite-spin part (V^2 + W^2)/D per unit
+    double* partial2;   // RESTRICTED: opposite-spin part per unit
 };
 
 namespace pair_f64_detail {
@@ -210,8 +210,10 @@ __global__ void __launch_bounds__(256, 2) pair_energy_f64_kernel(PairF64Args p) 
             const double w = (diag ? 1.0 : 2.0) * (i < j ? 2.0 : 1.0);
             sum.s *= w;
             sum.c *= w;
-            sum2.s *= w;
-            sum2.c *= w;
+            // opposite-spin part: sum over (a,b) and (b,a) of V_ab^2 is (V^2 + W^2)
+            // once per off-diagonal element, half of it on a diagonal block
+            sum2.s *= 0.5 * w;
+            sum2.c *= 0.5 * w;
         } else {
             const double w = diag ? 0.5 : 1.0;
             sum.s *= w;

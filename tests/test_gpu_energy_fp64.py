@@ -49,7 +49,7 @@ def test_closed_shell_unrestricted_vs_reference(ctx, golden, name):
     ctx.set_orbitals(capi.BETA, g["C"], g["eps"], o)
     e = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP64)
     assert close(e["ss_aa"], float(g["ump2_ss_aa"]), REL, 1e-13)
-    assert close(e["ss_bb"], float(g["ump2_ss_bb"]), REL, 1e-13)
+    assert close(e["ss_bb"], float(g.get("ump2_ss_bb", g["ump2_ss_aa"])), REL, 1e-13)
     assert close(e["os"], float(g["ump2_os"]))
     assert close(e["total"], float(g["e_corr"]), 1e-11)
 
