@@ -33,6 +33,8 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "cdrmp2_fp64_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
                                        precision="fp64", gradient=False),
+    "cdrmp2_bf16x3_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
+                                         precision="bf16x3", gradient=False),
 }
 DEFAULT_WORKLOAD = "cdrmp2_fp64_n400_o40_m1600"
 
@@ -87,7 +89,10 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, name):
+        setattr(self, name, time.time())
 
     def stop(self):
         if self.proc is None:
@@ -101,7 +106,12 @@ class ClockSampler:
             self._t.join(timeout=2)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples inside the timed window (widened by one sampling period on
+        # each side so that short windows still get the neighbouring samples)
+        t0 = getattr(self, "t_begin", 0.0) - 0.25
+        t1 = getattr(self, "t_end", float("inf")) + 0.25
+        window = [ln for (t, ln) in self.lines if t0 <= t <= t1]
+        for ln in window:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -249,8 +259,10 @@ def bench_gpu(args, w, rank, world, local_rank):
 
     clocks = ClockSampler(local_rank)
     clocks.start()
+    time.sleep(1.0)                      # nvidia-smi start-up
     barrier()
     torch.cuda.synchronize()
+    clocks.mark("t_begin")
     l0 = ctx.launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -263,7 +275,9 @@ def bench_gpu(args, w, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     launches = ctx.launch_count() - l0
+    clocks.mark("t_end")
     elapsed = ev0.elapsed_time(ev1) / 1e3
+    time.sleep(0.3)
     clk = clocks.stop()
 
     t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
@@ -336,7 +350,9 @@ def bench_gpu(args, w, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_elapsed / args.steps},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor", "kernel": "pair_energy_f64_kernel<RESTRICTED>",
+            "roofline": {"bound": "tensor",
+                         "kernel": ("pair_energy_f64_kernel<RESTRICTED>" if w["precision"] == "fp64"
+                                    else "pair_energy_tc_kernel<RESTRICTED>"),
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_note,
                          "kernel_ms": kms},

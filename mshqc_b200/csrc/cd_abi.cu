@@ -381,6 +381,7 @@ int mshqc_cd_set_orbitals(mshqc_cd_ctx* ctx, int spin, const double* C, const do
     s.nocc = nocc;
     s.set = true;
     s.invalidate();
+    ctx->diag_os_valid = false;
     CD_CUDA(cudaStreamSynchronize(ctx->stream));
     return MSHQC_CD_OK;
 }

@@ -36,9 +36,13 @@ struct SpinState {
     DevBuf B64;
     int64_t vp = 0;
     bool B64_valid = false;
-    // BF16 hi/lo split of the MO vectors for the tensor-core path
+    // fixed-point hi/lo (BF16 carriers) of the MO vectors for the tensor-core path
     DevBuf Bhi, Blo;
+    DevBuf expo;            // per-row power-of-two exponents [o][rows]
+    DevBuf diag;            // exact (ia|ia) [o][rows]
+    DevBuf norms;           // sum hi^2, sum lo^2 per row [2][o][rows]
     int64_t vp16 = 0, Mp16 = 0;
+    double max_norm_hi = 0, max_norm_lo = 0;
     bool B16_valid = false;
     void invalidate() {
         B64_valid = false;
@@ -76,18 +80,25 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf BT;            // backward: transposed MO vectors
     mshqc_cd::DevBuf W;             // backward: C_vir-contracted Gamma
     mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
+    mshqc_cd::DevBuf diag_os;       // sum_Q B_alpha[i][a] B_beta[i][a] (opposite-spin diagonal)
+    bool diag_os_valid = false;
+    int fixed_point_exact = 1;      // Cauchy-Schwarz bound of the last tensor-core pass held
 
     std::vector<double> pair_energy[3];  // host copies, row-major [i][j]
 
     void invalidate_all() {
         spin[0].invalidate();
         spin[1].invalidate();
+        diag_os_valid = false;
         for (auto& p : pair_energy) p.clear();
     }
     size_t held_bytes() const {
         size_t b = L.bytes + Y.bytes + scratch.bytes + tables.bytes + partial.bytes +
                    pair_sum.bytes + totals.bytes + flag.bytes + amp.bytes + BT.bytes + W.bytes;
-        for (const auto& s : spin) b += s.C.bytes + s.eps.bytes + s.B64.bytes + s.Bhi.bytes + s.Blo.bytes;
+        for (const auto& s : spin)
+            b += s.C.bytes + s.eps.bytes + s.B64.bytes + s.Bhi.bytes + s.Blo.bytes + s.expo.bytes +
+                 s.diag.bytes + s.norms.bytes;
+        b += diag_os.bytes;
         for (const auto& g : gam) b += g.bytes;
         for (const auto& g : grad) b += g.bytes;
         return b;
@@ -110,7 +121,11 @@ struct mshqc_cd_ctx {
             s.B64.release();
             s.Bhi.release();
             s.Blo.release();
+            s.expo.release();
+            s.diag.release();
+            s.norms.release();
         }
+        diag_os.release();
         for (auto& g : gam) g.release();
         for (auto& g : grad) g.release();
     }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -212,29 +213,77 @@ int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
 // ---------------------------------------------------------------------------
 // BF16x3 tensor-core path
 // ---------------------------------------------------------------------------
-int64_t tc_rows(int64_t v) {
-    const int64_t nblk = cdiv(v, 128);
-    return 128 * std::max<int64_t>(nblk + 1, round_up(nblk, 4));
-}
+int64_t tc_rows(int64_t v) { return 128 * round_up(cdiv(v, 128), 2); }
 
-// hi/lo BF16 split of one spin's FP64 MO vectors into the blocked layout
-int split_bf16(mshqc_cd_ctx* ctx, int spin) {
+// fixed-point hi/lo split of one spin's FP64 MO vectors into the blocked layout,
+// with the per-row exponents, exact diagonal integrals and hi/lo row norms
+int split_fixed(mshqc_cd_ctx* ctx, int spin) {
     SpinState& s = ctx->spin[spin];
     const int64_t o = s.nocc, v = ctx->N - s.nocc, M = ctx->M, Mp = ctx->Mp;
     const int64_t rows = tc_rows(v), nqc = Mp / 16;
     const size_t n = (size_t)o * nqc * rows * 16;
     CD_ALLOC(s.Bhi, n * sizeof(uint16_t), false);
     CD_ALLOC(s.Blo, n * sizeof(uint16_t), false);
+    CD_ALLOC(s.expo, sizeof(int) * o * rows, true);
+    CD_ALLOC(s.diag, sizeof(double) * o * rows, true);
+    CD_ALLOC(s.norms, sizeof(double) * 2 * o * rows, true);
     s.vp16 = rows;
     s.Mp16 = Mp;
-    const int64_t threads = o * nqc * rows * 2;
-    const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
-    split_bf16_blocked_kernel<<<blocks, 256, 0, ctx->stream>>>(
-        s.B64.as<double>(), s.vp, Mp, (int)v, (int)M, o, nqc, rows, s.Bhi.as<uint16_t>(),
-        s.Blo.as<uint16_t>());
+    double* nh = s.norms.as<double>();
+    double* nl = nh + o * rows;
+    {
+        const int64_t warps = o * rows;
+        const int blocks = (int)std::min<int64_t>(cdiv(warps * 32, 256), (int64_t)ctx->num_sms * 32);
+        row_scale_kernel<<<blocks, 256, 0, ctx->stream>>>(
+            s.B64.as<double>(), s.vp, Mp, (int)v, (int)M, o, rows, s.expo.as<int>(),
+            s.diag.as<double>(), nh, nl, nullptr, 0, 0, 0, nullptr);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+    }
+    {
+        const int64_t threads = o * nqc * rows * 2;
+        const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
+        split_fixed_blocked_kernel<<<blocks, 256, 0, ctx->stream>>>(
+            s.B64.as<double>(), s.vp, Mp, (int)v, (int)M, o, nqc, rows, s.expo.as<int>(),
+            s.Bhi.as<uint16_t>(), s.Blo.as<uint16_t>());
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+    }
+    // largest row norms: the Cauchy-Schwarz bound of the integer accumulators
+    std::vector<double> hn(2 * o * rows);
+    CD_CUDA(cudaMemcpyAsync(hn.data(), nh, sizeof(double) * 2 * o * rows, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    s.max_norm_hi = s.max_norm_lo = 0.0;
+    for (int64_t r = 0; r < o * rows; ++r) {
+        s.max_norm_hi = std::max(s.max_norm_hi, hn[r]);
+        s.max_norm_lo = std::max(s.max_norm_lo, hn[o * rows + r]);
+    }
+    s.B16_valid = true;
+    return MSHQC_CD_OK;
+}
+
+// exact sum_Q B_alpha[i][a][Q] B_beta[i][a][Q] for the opposite-spin diagonal
+int opposite_spin_diag(mshqc_cd_ctx* ctx) {
+    if (ctx->diag_os_valid) return MSHQC_CD_OK;
+    SpinState& A = ctx->spin[0];
+    SpinState& B = ctx->spin[1];
+    const int64_t oa = A.nocc, va = ctx->N - A.nocc, rows = A.vp16;
+    const int o2 = (int)std::min(A.nocc, B.nocc);
+    const int v2 = (int)std::min(ctx->N - A.nocc, ctx->N - B.nocc);
+    CD_ALLOC(ctx->diag_os, sizeof(double) * std::max<int64_t>(1, (int64_t)o2 * rows), true);
+    CD_ALLOC(ctx->scratch, sizeof(double) * (size_t)(oa * rows * 4), false);
+    double* tmp = ctx->scratch.as<double>();
+    int* etmp = reinterpret_cast<int*>(tmp + 3 * oa * rows);
+    const int64_t warps = oa * rows;
+    const int blocks = (int)std::min<int64_t>(cdiv(warps * 32, 256), (int64_t)ctx->num_sms * 32);
+    row_scale_kernel<<<blocks, 256, 0, ctx->stream>>>(
+        A.B64.as<double>(), A.vp, ctx->Mp, (int)va, (int)ctx->M, oa, rows, etmp, tmp,
+        tmp + oa * rows, tmp + 2 * oa * rows, B.B64.as<double>(), B.vp, o2, v2,
+        ctx->diag_os.as<double>());
     CD_CUDA(cudaGetLastError());
     ctx->launches++;
-    s.B16_valid = true;
+    ctx->diag_os_valid = true;
     return MSHQC_CD_OK;
 }
 
@@ -244,13 +293,13 @@ UnitTables make_tables_tc(int mode, int ox, int oy, int nbx, int nby) {
         for (int i = 0; i < ox; ++i)
             for (int j = 0; j < oy; ++j) t.pairs.push_back(make_int2(i, j));
         for (int x = 0; x < nbx; ++x)
-            for (int y = 0; y < nby; y += 4) t.blocks.push_back(make_int2(x, y));
+            for (int y = 0; y < nby; y += 2) t.blocks.push_back(make_int2(x, y));
     } else {
         for (int i = 0; i < ox; ++i)
             for (int j = (mode == PAIR_RESTRICTED ? i : i + 1); j < ox; ++j)
                 t.pairs.push_back(make_int2(i, j));
         for (int x = 0; x < nbx; ++x)
-            for (int y = x; y < nbx; y += 2) t.blocks.push_back(make_int2(x, y));
+            for (int y = x; y < nbx; ++y) t.blocks.push_back(make_int2(x, y));
     }
     return t;
 }
@@ -292,9 +341,29 @@ int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
     CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
 
+    // the integer accumulators are exact when every partial sum stays below
+    // 2^24: |sum hi hi'| <= sqrt(max sum hi^2 * max sum hi'^2), likewise for
+    // the cross terms (Cauchy-Schwarz over the Q index)
+    {
+        const double lim = 16777216.0;
+        const double bhh = std::sqrt(X.max_norm_hi * Y.max_norm_hi);
+        const double bx = std::sqrt(X.max_norm_hi * Y.max_norm_lo) + std::sqrt(X.max_norm_lo * Y.max_norm_hi);
+        if (!(bhh < lim && bx < lim)) ctx->fixed_point_exact = 0;
+    }
+    if (mode == PAIR_OPPOSITE_SPIN) CD_RC(opposite_spin_diag(ctx));
     PairTcArgs a{};
     a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
     a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
+    a.ex = X.expo.as<int>();  a.ey = Y.expo.as<int>();
+    if (mode == PAIR_OPPOSITE_SPIN) {
+        a.diag = ctx->diag_os.as<double>();
+        a.diag_o = (int)std::min(X.nocc, Y.nocc);
+        a.diag_v = std::min(vx, vy);
+    } else {
+        a.diag = X.diag.as<double>();
+        a.diag_o = ox;
+        a.diag_v = vx;
+    }
     a.rows_x = (int)X.vp16;  a.rows_y = (int)Y.vp16;
     a.nqc = (int)(ctx->Mp / 16);
     a.vx = vx;  a.vy = vy;
@@ -335,12 +404,13 @@ int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
         CD_RC(transform_f64(ctx, spin));
         s.B16_valid = false;
     }
-    if (precision == MSHQC_CD_BF16X3 && !s.B16_valid) CD_RC(split_bf16(ctx, spin));
+    if (precision == MSHQC_CD_BF16X3 && !s.B16_valid) CD_RC(split_fixed(ctx, spin));
     return MSHQC_CD_OK;
 }
 
 int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out) {
     std::memset(out, 0, sizeof(*out));
+    ctx->fixed_point_exact = 1;
     auto pass = [&](int mode, int sx, int sy, double* tot, std::vector<double>& pm,
                     double* tot_os) {
         return precision == MSHQC_CD_BF16X3 ? pair_pass_tc(ctx, mode, sx, sy, tot, pm, tot_os)

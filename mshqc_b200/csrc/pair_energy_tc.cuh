@@ -1,47 +1,53 @@
-// Fused BF16x3 pair-energy kernel on the 5th-generation tensor cores (tcgen05).
+// Fused pair-energy kernel on the 5th-generation tensor cores (tcgen05), exact
+// fixed-point accumulation (split_bf16.cuh describes the hi/lo encoding).
 //
-// Operands: the MO vectors split as B = hi + lo (both BF16), stored in a
-// "core-matrix blocked" layout so that every operand slab is one contiguous
-// run of bytes and lands in shared memory already in the canonical K-major
-// no-swizzle UMMA layout:
+// Operands live in a "core-matrix blocked" layout so that every operand slab
+// is one contiguous run of bytes that lands in shared memory already in the
+// canonical K-major no-swizzle UMMA layout:
 //
 //   element (i, a, Q) at  (i*nqc + Q/16)*rows*16 + (a/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
 //
-// (rows = allocated virtual rows per occupied orbital, a multiple of 128 plus
-// one spare block of zeros).  A slab = rows [a0, a0+R) x Q-chunk of 16 =
-// R*32 contiguous bytes.
+// A slab = rows [a0, a0+128) x one 16-wide Q chunk = 4 KB contiguous.
 //
-// One work unit = pair (i,j), virtual row block x (128 rows of a), column
-// range starting at 128-block y (256 columns of b).  Per 16-wide Q step the
-// MMA warp issues six 128x256x16 MMAs accumulating in TMEM:
-//   T1 (cols 0..255)   += Xhi_i[x] Yhi_j[y]^T + Xhi_i[x] Ylo_j[y]^T + Xlo_i[x] Yhi_j[y]^T
-//   T2 (cols 256..511) += (same with slabs P2, P3)
-// RESTRICTED / SAME_SPIN: T1 = (ia|jb), T2 = (ib|ja) at the same (a,b);
-// OPPOSITE_SPIN: T1, T2 = (ia|jb) for column ranges y and y+2 (blocks of 128).
-// The epilogue warps read the accumulators with tcgen05.ld, form the FP64
-// denominators and reduce the energy of the unit into partial[unit] (FP64)
-// without ever writing (ia|jb) or the amplitudes to memory.  Element weights
-// and formulas are those of the FP64 kernel (pair_energy_f64.cuh).
+// Work unit = pair (i,j), row block x (128 virtuals a), column block y (128
+// virtuals b).  Per Q chunk the MMA thread issues six 128x128x16 MMAs into
+// four TMEM accumulators (columns):
+//   [  0,128) T1hh = Xhi_i[x] . Yhi_j[y]
+//   [128,256) T1x  = Xhi_i[x] . Ylo_j[y] + Xlo_i[x] . Yhi_j[y]
+//   [256,384) T2hh, [384,512) T2x   the same for slabs P2, P3
+// RESTRICTED / SAME_SPIN: P2 = X_j[x], P3 = X_i[y]  ->  T2 = (ib|ja) at (a,b);
+// OPPOSITE_SPIN: P2 = P0, P3 = Y_j[y+1]            ->  T2 = (ia|jb') of the next block.
+// All accumulator entries are exact integers, so the epilogue recovers
+//   (ia|jb) = u_ia u_jb (T1hh + T1x / 256)
+// exactly in FP64, substitutes the exact FP64 (ia|ia) on the diagonal, forms
+// FP64 denominators and reduces the unit's energy (weights and formulas of
+// pair_energy_f64.cuh) into partial[unit].  (ia|jb) and the amplitudes are
+// never written to memory.
 //
 // Warp roles (192 threads): warp 0 producer (bulk copies), warp 1 MMA issuer
 // and TMEM owner, warps 2..5 epilogue (TMEM lane quadrant = warp % 4).
 // Every wait is bounded (kWaitLimitNs); on a timeout the kernel records the
-// place in *err, drains its own copies and MMAs (again bounded), frees TMEM and
+// site in *err, drains its own copies and MMAs (again bounded), frees TMEM and
 // returns.
 #pragma once
 
 #include "cd_common.cuh"
 #include "pair_energy_f64.cuh"
 #include "sm100_ptx.cuh"
+#include "split_bf16.cuh"
 
 namespace mshqc_cd {
 
 struct PairTcArgs {
-    const uint16_t* Xhi; const uint16_t* Xlo;   // blocked BF16 bits, spin X
+    const uint16_t* Xhi; const uint16_t* Xlo;   // blocked FP16 bits, spin X
     const uint16_t* Yhi; const uint16_t* Ylo;   // spin Y (== X for RESTRICTED / SAME_SPIN)
-    int rows_x, rows_y;     // allocated rows per occupied orbital (multiple of 128, + 128 spare)
+    const int* ex; const int* ey;               // row exponents [o][rows]
+    const double* diag;                         // exact (ia|ia): [ox][rows_x] (RESTRICTED)
+                                                // or sum_Q Xa*Yb [diag_o][rows_x] (OPPOSITE)
+    int rows_x, rows_y;     // allocated rows per occupied orbital
     int nqc;                // number of 16-wide Q chunks
     int vx, vy;             // virtual counts
+    int diag_o, diag_v;     // extent of the opposite-spin diagonal table
     const double* eox; const double* evx;
     const double* eoy; const double* evy;
     const int2* pairs;      // (i, j)
@@ -50,26 +56,33 @@ struct PairTcArgs {
     long long units;        // npairs * nblocks
     double* partial;        // [units]
     double* partial2;       // [units] RESTRICTED opposite-spin part
-    int* err;               // nonzero after a timeout
+    int* err;               // err[0]: nonzero after a timeout; err[1]: an accumulator reached 2^24
 };
 
 namespace pair_tc {
 constexpr int BM = 128;
-constexpr int BN = 256;
+constexpr int BN = 128;
 constexpr int KC = 16;
-constexpr int STAGES = 4;
+constexpr int STAGES = 6;
 constexpr int THREADS = 192;
-constexpr uint32_t SLAB_A = BM * KC * 2;   // 4096 bytes
-constexpr uint32_t SLAB_B = BN * KC * 2;   // 8192 bytes
+constexpr uint32_t SLAB = 128 * KC * 2;    // 4096 bytes
 // stage layout: P0hi P1hi P2hi P3hi P0lo P1lo P2lo P3lo
-constexpr uint32_t OFF_P0 = 0, OFF_P1 = SLAB_A, OFF_P2 = SLAB_A + SLAB_B, OFF_P3 = 2 * SLAB_A + SLAB_B;
-constexpr uint32_t HALF = 2 * (SLAB_A + SLAB_B);           // 24576
-constexpr uint32_t STAGE_BYTES = 2 * HALF;                  // 49152
-constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;        // 196608
-constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 /*align*/ + 512 /*barriers, eps*/ + BN * 2 * 8;
-constexpr uint64_t kWaitLimitNs = 2000000000ull;            // 2 s
+constexpr uint32_t HALF = 4 * SLAB;                          // 16384
+constexpr uint32_t STAGE_BYTES = 2 * HALF;                   // 32768
+constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;         // 196608
+// after the data: barriers (< 256 B), reduction scratch (64 B at +256),
+// per-unit column tables at +512: eps (2 x 128 doubles), column scales
+// (2 x 128 doubles)
+constexpr uint32_t OFF_AUX = 512;
+constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 /*align*/ + OFF_AUX + 4 * 128 * 8;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;             // 2 s
 constexpr uint32_t TMEM_COLS = 512;
 }  // namespace pair_tc
+
+// 2^e as a double (|e| well inside the normal range)
+__device__ __forceinline__ double pow2d(int e) {
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
@@ -84,8 +97,9 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
     uint64_t* drain = tmem_empty + 1;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    double* red = reinterpret_cast<double*>(smem + SMEM_DATA + 128);        // 2 x 4 warps
-    double* eb_s = reinterpret_cast<double*>(smem + SMEM_DATA + 512);       // 2 x 256
+    double* red = reinterpret_cast<double*>(smem + SMEM_DATA + 256);           // 8 doubles
+    double* eb_s = reinterpret_cast<double*>(smem + SMEM_DATA + OFF_AUX);      // 256
+    double* cs_s = eb_s + 256;                                                 // 256
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -124,24 +138,26 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                 const int2 ij = p.pairs[u / p.nblocks];
                 const int2 xy = p.blocks[u % p.nblocks];
                 const size_t rx = p.rows_x, ry = p.rows_y;
-                const uint16_t *p0h, *p1h, *p2h, *p3h, *p0l, *p1l, *p2l, *p3l;
-                // slab bases at Q-chunk 0; chunk qc adds qc * rows * 16 elements
-                const size_t a0 = (size_t)xy.x * BM, b0 = (size_t)xy.y * 128;
+                const size_t a0 = (size_t)xy.x * BM, b0 = (size_t)xy.y * BN;
+                // slab bases at Q chunk 0; chunk kq adds kq * rows * 16 elements
+                const uint16_t *s0h, *s1h, *s2h, *s3h, *s0l, *s1l, *s2l, *s3l;
+                size_t c0, c1, c2, c3;
                 if (MODE == PAIR_OPPOSITE_SPIN) {
                     const size_t oi = (size_t)ij.x * p.nqc * rx * 16, oj = (size_t)ij.y * p.nqc * ry * 16;
-                    p0h = p.Xhi + oi + a0 * 16;  p0l = p.Xlo + oi + a0 * 16;
-                    p1h = p.Yhi + oj + b0 * 16;  p1l = p.Ylo + oj + b0 * 16;
-                    p2h = p0h;                   p2l = p0l;
-                    p3h = p.Yhi + oj + (b0 + BN) * 16;  p3l = p.Ylo + oj + (b0 + BN) * 16;
+                    s0h = p.Xhi + oi + a0 * 16;         s0l = p.Xlo + oi + a0 * 16;
+                    s1h = p.Yhi + oj + b0 * 16;         s1l = p.Ylo + oj + b0 * 16;
+                    s2h = s0h;                          s2l = s0l;
+                    s3h = p.Yhi + oj + (b0 + BN) * 16;  s3l = p.Ylo + oj + (b0 + BN) * 16;
+                    c0 = rx * 16; c1 = ry * 16; c2 = c0; c3 = ry * 16;
                 } else {
                     const size_t oi = (size_t)ij.x * p.nqc * rx * 16, oj = (size_t)ij.y * p.nqc * rx * 16;
-                    p0h = p.Xhi + oi + a0 * 16;  p0l = p.Xlo + oi + a0 * 16;
-                    p1h = p.Xhi + oj + b0 * 16;  p1l = p.Xlo + oj + b0 * 16;
-                    p2h = p.Xhi + oj + a0 * 16;  p2l = p.Xlo + oj + a0 * 16;
-                    p3h = p.Xhi + oi + b0 * 16;  p3l = p.Xlo + oi + b0 * 16;
+                    s0h = p.Xhi + oi + a0 * 16;  s0l = p.Xlo + oi + a0 * 16;
+                    s1h = p.Xhi + oj + b0 * 16;  s1l = p.Xlo + oj + b0 * 16;
+                    s2h = p.Xhi + oj + a0 * 16;  s2l = p.Xlo + oj + a0 * 16;
+                    s3h = p.Xhi + oi + b0 * 16;  s3l = p.Xlo + oi + b0 * 16;
+                    c0 = c1 = c2 = c3 = rx * 16;
                 }
-                const size_t cx = rx * 16, cy = (MODE == PAIR_OPPOSITE_SPIN) ? ry * 16 : rx * 16;
-                const uint32_t bytes = (MODE == PAIR_OPPOSITE_SPIN) ? 2 * (SLAB_A + 2 * SLAB_B) : STAGE_BYTES;
+                const uint32_t bytes = (MODE == PAIR_OPPOSITE_SPIN) ? 6 * SLAB : 8 * SLAB;
                 for (int kq = 0; kq < nk; ++kq) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
                         atomicExch(p.err, 1);
@@ -150,20 +166,17 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                     }
                     uint8_t* sb = smem + stage * STAGE_BYTES;
                     mbar_arrive_expect_tx(&full[stage], bytes);
-                    const size_t qx = (size_t)kq * cx, qy = (size_t)kq * cy;
-                    bulk_g2s(sb + OFF_P0, p0h + qx, SLAB_A, &full[stage]);
-                    bulk_g2s(sb + HALF + OFF_P0, p0l + qx, SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_P1, p1h + qy, SLAB_B, &full[stage]);
-                    bulk_g2s(sb + HALF + OFF_P1, p1l + qy, SLAB_B, &full[stage]);
+                    const size_t k = (size_t)kq;
+                    bulk_g2s(sb + 0 * SLAB, s0h + k * c0, SLAB, &full[stage]);
+                    bulk_g2s(sb + HALF + 0 * SLAB, s0l + k * c0, SLAB, &full[stage]);
+                    bulk_g2s(sb + 1 * SLAB, s1h + k * c1, SLAB, &full[stage]);
+                    bulk_g2s(sb + HALF + 1 * SLAB, s1l + k * c1, SLAB, &full[stage]);
                     if (MODE != PAIR_OPPOSITE_SPIN) {
-                        bulk_g2s(sb + OFF_P2, p2h + qy, SLAB_A, &full[stage]);
-                        bulk_g2s(sb + HALF + OFF_P2, p2l + qy, SLAB_A, &full[stage]);
-                        bulk_g2s(sb + OFF_P3, p3h + qx, SLAB_B, &full[stage]);
-                        bulk_g2s(sb + HALF + OFF_P3, p3l + qx, SLAB_B, &full[stage]);
-                    } else {
-                        bulk_g2s(sb + OFF_P3, p3h + qy, SLAB_B, &full[stage]);
-                        bulk_g2s(sb + HALF + OFF_P3, p3l + qy, SLAB_B, &full[stage]);
+                        bulk_g2s(sb + 2 * SLAB, s2h + k * c2, SLAB, &full[stage]);
+                        bulk_g2s(sb + HALF + 2 * SLAB, s2l + k * c2, SLAB, &full[stage]);
                     }
+                    bulk_g2s(sb + 3 * SLAB, s3h + k * c3, SLAB, &full[stage]);
+                    bulk_g2s(sb + HALF + 3 * SLAB, s3l + k * c3, SLAB, &full[stage]);
                     fill_phase[stage] = phase;
                     filled[stage] = true;
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
@@ -188,7 +201,7 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
-            constexpr uint32_t IDESC = idesc_bf16_f32(BM, BN);
+            constexpr uint32_t IDESC = idesc_f16_f32(BM, BN);
             uint32_t stage = 0, phase = 0, acc_phase = 0;
             const uint32_t sbase = smem_addr(smem);
             for (long long u = first; u < p.units && !*abort_flag; u += step) {
@@ -208,21 +221,21 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                     }
                     tc_fence_after();
                     const uint32_t sb = sbase + stage * STAGE_BYTES;
-                    const uint64_t a0h = smem_desc_kmajor(sb + OFF_P0, 128, 256);
-                    const uint64_t a0l = smem_desc_kmajor(sb + HALF + OFF_P0, 128, 256);
-                    const uint64_t b1h = smem_desc_kmajor(sb + OFF_P1, 128, 256);
-                    const uint64_t b1l = smem_desc_kmajor(sb + HALF + OFF_P1, 128, 256);
-                    const uint32_t accum = kq > 0 ? 1u : 0u;
-                    mma_bf16(tmem, a0h, b1h, IDESC, accum);
-                    mma_bf16(tmem, a0h, b1l, IDESC, 1u);
-                    mma_bf16(tmem, a0l, b1h, IDESC, 1u);
-                    const uint64_t a2h = (MODE == PAIR_OPPOSITE_SPIN) ? a0h : smem_desc_kmajor(sb + OFF_P2, 128, 256);
-                    const uint64_t a2l = (MODE == PAIR_OPPOSITE_SPIN) ? a0l : smem_desc_kmajor(sb + HALF + OFF_P2, 128, 256);
-                    const uint64_t b3h = smem_desc_kmajor(sb + OFF_P3, 128, 256);
-                    const uint64_t b3l = smem_desc_kmajor(sb + HALF + OFF_P3, 128, 256);
-                    mma_bf16(tmem + BN, a2h, b3h, IDESC, accum);
-                    mma_bf16(tmem + BN, a2h, b3l, IDESC, 1u);
-                    mma_bf16(tmem + BN, a2l, b3h, IDESC, 1u);
+                    const uint64_t p0h = smem_desc_kmajor(sb + 0 * SLAB, 128, 256);
+                    const uint64_t p1h = smem_desc_kmajor(sb + 1 * SLAB, 128, 256);
+                    const uint64_t p3h = smem_desc_kmajor(sb + 3 * SLAB, 128, 256);
+                    const uint64_t p0l = smem_desc_kmajor(sb + HALF + 0 * SLAB, 128, 256);
+                    const uint64_t p1l = smem_desc_kmajor(sb + HALF + 1 * SLAB, 128, 256);
+                    const uint64_t p3l = smem_desc_kmajor(sb + HALF + 3 * SLAB, 128, 256);
+                    const uint64_t p2h = (MODE == PAIR_OPPOSITE_SPIN) ? p0h : smem_desc_kmajor(sb + 2 * SLAB, 128, 256);
+                    const uint64_t p2l = (MODE == PAIR_OPPOSITE_SPIN) ? p0l : smem_desc_kmajor(sb + HALF + 2 * SLAB, 128, 256);
+                    const uint32_t acc = kq > 0 ? 1u : 0u;
+                    mma_f16(tmem + 0, p0h, p1h, IDESC, acc);
+                    mma_f16(tmem + 128, p0h, p1l, IDESC, acc);
+                    mma_f16(tmem + 128, p0l, p1h, IDESC, 1u);
+                    mma_f16(tmem + 256, p2h, p3h, IDESC, acc);
+                    mma_f16(tmem + 384, p2h, p3l, IDESC, acc);
+                    mma_f16(tmem + 384, p2l, p3h, IDESC, 1u);
                     mma_commit(&empty[stage]);       // frees the stage when these MMAs finish
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
@@ -243,14 +256,29 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             if (*abort_flag) break;
             const int2 ij = p.pairs[u / p.nblocks];
             const int2 xy = p.blocks[u % p.nblocks];
+            const int i = ij.x, j = ij.y;
             const int a = xy.x * BM + row;
-            const int bbase = xy.y * 128;
-            // stage the column energies of this unit while the MMAs run
+            const int b0 = xy.y * BN;
+            // per-unit column tables (eps and scales of T1 / T2 columns)
             for (int c = etid; c < 2 * BN; c += 128) {
-                const int b = bbase + c;
-                const int lim = (MODE == PAIR_OPPOSITE_SPIN) ? p.vy : p.vx;
-                const double* ev = (MODE == PAIR_OPPOSITE_SPIN) ? p.evy : p.evx;
-                eb_s[c] = (b < lim && (MODE == PAIR_OPPOSITE_SPIN || c < BN)) ? ev[b] : 0.0;
+                const int half = c / BN, cc = c % BN;
+                double eb = 0.0, cs = 0.0;
+                if (MODE == PAIR_OPPOSITE_SPIN) {
+                    const int b = b0 + half * BN + cc;
+                    if (b < p.vy) {
+                        eb = p.evy[b];
+                        cs = pow2d(p.ey[(size_t)j * p.rows_y + b] - kFixedHiBits);
+                    }
+                } else {
+                    const int b = b0 + cc;
+                    if (b < p.vx) {
+                        eb = p.evx[b];
+                        // T1 columns are rows of X_j, T2 columns rows of X_i
+                        cs = pow2d(p.ex[(size_t)(half == 0 ? j : i) * p.rows_x + b] - kFixedHiBits);
+                    }
+                }
+                eb_s[c] = eb;
+                cs_s[c] = cs;
             }
             asm volatile("bar.sync 1, 128;\n" ::: "memory");
             if (!mbar_wait_bounded(tmem_full, acc_phase, kWaitLimitNs)) {
@@ -262,54 +290,70 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             tc_fence_after();
 
             const bool arow = a < p.vx;
-            double s_lo = 0.0, s_hi = 0.0, o_lo = 0.0, o_hi = 0.0;   // per column half
-            const double eij = (MODE == PAIR_OPPOSITE_SPIN) ? p.eox[ij.x] + p.eoy[ij.y]
-                                                            : p.eox[ij.x] + p.eox[ij.y];
-            const double ta = arow ? eij - p.evx[a] : 0.0;
+            double rs1 = 0.0, rs2 = 0.0, ta = 0.0, dg1 = 0.0, dg2 = 0.0;
+            int dcol1 = -1, dcol2 = -1;   // column holding a == b (exact diagonal), if any
+            if (arow) {
+                if (MODE == PAIR_OPPOSITE_SPIN) {
+                    rs1 = rs2 = pow2d(p.ex[(size_t)i * p.rows_x + a] - kFixedHiBits);
+                    ta = p.eox[i] + p.eoy[j] - p.evx[a];
+                    if (i == j && i < p.diag_o && a < p.diag_v) {
+                        const int c1 = a - b0, c2 = a - b0 - BN;
+                        if (c1 >= 0 && c1 < BN) { dcol1 = c1; dg1 = p.diag[(size_t)i * p.rows_x + a]; }
+                        if (c2 >= 0 && c2 < BN) { dcol2 = c2; dg2 = p.diag[(size_t)i * p.rows_x + a]; }
+                    }
+                } else {
+                    rs1 = pow2d(p.ex[(size_t)i * p.rows_x + a] - kFixedHiBits);
+                    rs2 = pow2d(p.ex[(size_t)j * p.rows_x + a] - kFixedHiBits);
+                    ta = p.eox[i] + p.eox[j] - p.evx[a];
+                    if (MODE == PAIR_RESTRICTED && i == j && a >= b0 && a < b0 + BN) {
+                        dcol1 = dcol2 = a - b0;
+                        dg1 = dg2 = p.diag[(size_t)i * p.rows_x + a];
+                    }
+                }
+            }
+            double s_acc = 0.0, o_acc = 0.0;
+            float amax = 0.0f;
             const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 32) {
-                uint32_t r1[32], r2[32];
-                tmem_ld32(lane_base + c0, r1);
-                tmem_ld32(lane_base + BN + c0, r2);
+                uint32_t h1[32], x1[32], h2[32], x2[32];
+                tmem_ld32(lane_base + 0 + c0, h1);
+                tmem_ld32(lane_base + 128 + c0, x1);
+                tmem_ld32(lane_base + 256 + c0, h2);
+                tmem_ld32(lane_base + 384 + c0, x2);
                 tmem_ld_wait();
                 if (!arow) continue;
-                const bool hi_half = c0 >= 128;
 #pragma unroll
                 for (int k = 0; k < 32; ++k) {
                     const int c = c0 + k;
-                    const float V = __uint_as_float(r1[k]);
-                    const float W = __uint_as_float(r2[k]);
+                    amax = fmaxf(amax, fmaxf(fmaxf(fabsf(__uint_as_float(h1[k])), fabsf(__uint_as_float(x1[k]))),
+                                             fmaxf(fabsf(__uint_as_float(h2[k])), fabsf(__uint_as_float(x2[k])))));
+                    double v1 = fma((double)__uint_as_float(x1[k]), 1.0 / kFixedLoScale,
+                                    (double)__uint_as_float(h1[k])) * (rs1 * cs_s[c]);
+                    double v2 = fma((double)__uint_as_float(x2[k]), 1.0 / kFixedLoScale,
+                                    (double)__uint_as_float(h2[k])) * (rs2 * cs_s[BN + c]);
+                    if (c == dcol1) v1 = dg1;
+                    if (c == dcol2) v2 = dg2;
                     if (MODE == PAIR_OPPOSITE_SPIN) {
-                        if (bbase + c < p.vy) {
+                        if (b0 + c < p.vy) {
                             const double D = ta - eb_s[c];
-                            if (fabs(D) >= kDenomSkip) {
-                                const double t = (double)(V * V) * recip_nr(D);
-                                if (hi_half) s_hi += t; else s_lo += t;
-                            }
+                            if (fabs(D) >= kDenomSkip) s_acc = fma(v1 * v1, recip_nr(D), s_acc);
                         }
-                        if (bbase + BN + c < p.vy) {
+                        if (b0 + BN + c < p.vy) {
                             const double D = ta - eb_s[BN + c];
-                            if (fabs(D) >= kDenomSkip) {
-                                const double t = (double)(W * W) * recip_nr(D);
-                                if (hi_half) o_hi += t; else o_lo += t;
-                            }
+                            if (fabs(D) >= kDenomSkip) s_acc = fma(v2 * v2, recip_nr(D), s_acc);
                         }
-                    } else {
-                        if (bbase + c < p.vx) {
-                            const double D = ta - eb_s[c];
-                            if (fabs(D) >= kDenomSkip) {
-                                const double rD = recip_nr(D);
-                                if (MODE == PAIR_RESTRICTED) {
-                                    const float vw = fmaf(V, V, fmaf(W, W, -V * W));
-                                    const float os = fmaf(V, V, W * W);
-                                    if (hi_half) { s_hi += (double)vw * rD; o_hi += (double)os * rD; }
-                                    else         { s_lo += (double)vw * rD; o_lo += (double)os * rD; }
-                                } else {
-                                    const float g = V - W;
-                                    const double t = (double)(g * g) * rD;
-                                    if (hi_half) s_hi += t; else s_lo += t;
-                                }
+                    } else if (b0 + c < p.vx) {
+                        const double D = ta - eb_s[c];
+                        if (fabs(D) >= kDenomSkip) {
+                            const double rD = recip_nr(D);
+                            if (MODE == PAIR_RESTRICTED) {
+                                const double sq = fma(v1, v1, v2 * v2);
+                                s_acc = fma(fma(-v1, v2, sq), rD, s_acc);
+                                o_acc = fma(sq, rD, o_acc);
+                            } else {
+                                const double g = v1 - v2;
+                                s_acc = fma(g * g, rD, s_acc);
                             }
                         }
                     }
@@ -317,26 +361,21 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             }
             // accumulators consumed: hand TMEM back to the MMA warp
             tc_fence_before();
+            __syncwarp();
             if (lane == 0) mbar_arrive(tmem_empty);
+            if (amax >= 16777216.0f) atomicOr(p.err + 1, 1);
 
-            // weights: column block z = y (first 128) / y+1 (second 128) vs row block x
-            double tot1, tot2;
-            if (MODE == PAIR_OPPOSITE_SPIN) {
-                tot1 = (s_lo + s_hi) + (o_lo + o_hi);
-                tot2 = 0.0;
-            } else {
-                const int x = xy.x, z0 = xy.y, z1 = xy.y + 1;
-                double w0, w1;
+            // unit weights (see pair_energy_f64.cuh)
+            double tot1 = s_acc, tot2 = 0.0;
+            if (MODE != PAIR_OPPOSITE_SPIN) {
+                const bool diagblk = (xy.x == xy.y);
                 if (MODE == PAIR_RESTRICTED) {
-                    const double wp = ij.x < ij.y ? 2.0 : 1.0;
-                    w0 = wp * (z0 == x ? 1.0 : 2.0);
-                    w1 = wp * (z1 == x ? 1.0 : 2.0);
+                    const double w = (diagblk ? 1.0 : 2.0) * (i < j ? 2.0 : 1.0);
+                    tot1 = w * s_acc;
+                    tot2 = 0.5 * w * o_acc;
                 } else {
-                    w0 = (z0 == x ? 0.5 : 1.0);
-                    w1 = (z1 == x ? 0.5 : 1.0);
+                    tot1 = (diagblk ? 0.5 : 1.0) * s_acc;
                 }
-                tot1 = w0 * s_lo + w1 * s_hi;
-                tot2 = 0.5 * (w0 * o_lo + w1 * o_hi);
             }
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {

@@ -85,8 +85,8 @@ __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 }
 
-// D[tmem] (+)= A[smem] * B[smem]^T, kind::f16 (bf16 inputs here), issued by one thread.
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+// D[tmem] (+)= A[smem] * B[smem]^T, kind::f16 (16-bit inputs, type in idesc), one thread.
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -117,6 +117,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 }
 __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Instruction descriptor, kind::f16: FP16 x FP16 -> FP32, both operands K-major.
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
+    return (1u << 4)                        // D format: F32; A, B format 0: F16
+           | ((uint32_t)(N >> 3) << 17)     // N / 8
+           | ((uint32_t)(M >> 4) << 24);    // M / 16
 }
 
 // Instruction descriptor, kind::f16: BF16 x BF16 -> FP32, both operands K-major.
