@@ -33,8 +33,8 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "cdrmp2_fp64_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
                                        precision="fp64", gradient=False),
-    "cdrmp2_bf16x3_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
-                                         precision="bf16x3", gradient=False),
+    "cdrmp2_fp16x3_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
+                                         precision="fp16x3", gradient=False),
 }
 DEFAULT_WORKLOAD = "cdrmp2_fp64_n400_o40_m1600"
 
@@ -338,7 +338,7 @@ def bench_gpu(args, w, rank, world, local_rank):
             "metric": metric_name(w), "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if w["precision"] == "fp64" else "bf16x3/f32 (f64 denominators, sums)",
+            "dtype": "f64" if w["precision"] == "fp64" else "fp16x3 (scaled fixed point, exact f32 accumulate; f64 denominators, sums)",
             "data": "synthetic",
             "config": {"workload": args.workload, "N": N, "o": o, "v": N - o, "M": M,
                        "kind": w["kind"], "precision": w["precision"],

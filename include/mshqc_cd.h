@@ -53,9 +53,12 @@ enum mshqc_cd_status {
 };
 
 enum mshqc_cd_precision {
-    MSHQC_CD_FP64 = 0,   /* FP64 contractions (DMMA)                        */
-    MSHQC_CD_BF16X3 = 1  /* hi/lo BF16 split, 3 products, FP32 accumulate on
-                            the tensor cores; FP64 denominators and energies */
+    MSHQC_CD_FP64 = 0,    /* FP64 contractions (DMMA)                       */
+    MSHQC_CD_FP16X3 = 1   /* scaled FP16 x3: every MO row in fixed point with
+                             one power-of-two scale, integer hi/lo carried in
+                             FP16, three products per pair, exact FP32
+                             accumulation on the tensor cores; FP64
+                             denominators, diagonal integrals and energies  */
 };
 
 enum mshqc_cd_kind {

@@ -19,13 +19,13 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "mshqc_cd.h")
 OK = 0
 ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_NUMERIC, ERR_UNSUPPORTED, ERR_TIMEOUT = (
     -1, -2, -3, -4, -5, -6, -7)
-FP64, BF16X3 = 0, 1
+FP64, FP16X3 = 0, 1
 RESTRICTED, UNRESTRICTED = 0, 1
 LAYOUT_FULL, LAYOUT_PACKED = 0, 1
 HOST, DEVICE = 0, 1
 ALPHA, BETA = 0, 1
 
-PRECISIONS = {"fp64": FP64, "bf16x3": BF16X3}
+PRECISIONS = {"fp64": FP64, "fp16x3": FP16X3}
 
 
 class CDError(RuntimeError):

@@ -417,7 +417,7 @@ int mshqc_cd_mp2_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_ene
     if (!out) return set_error(MSHQC_CD_ERR_ARG, "out is null");
     if (kind != MSHQC_CD_RESTRICTED && kind != MSHQC_CD_UNRESTRICTED)
         return set_error(MSHQC_CD_ERR_ARG, "unknown kind");
-    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_BF16X3)
+    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_FP16X3)
         return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
     DeviceGuard g(ctx->device);
     return run_energy(ctx, kind, precision, out);
@@ -443,7 +443,7 @@ int mshqc_cd_mp2_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_e
     CD_CHECK_CTX();
     if (kind != MSHQC_CD_RESTRICTED && kind != MSHQC_CD_UNRESTRICTED)
         return set_error(MSHQC_CD_ERR_ARG, "unknown kind");
-    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_BF16X3)
+    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_FP16X3)
         return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
     DeviceGuard g(ctx->device);
     return run_gradient(ctx, kind, precision, e_out, dC_a, dC_b, deps_a, deps_b, where);

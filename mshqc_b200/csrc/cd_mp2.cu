@@ -211,7 +211,7 @@ int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
 
 
 // ---------------------------------------------------------------------------
-// BF16x3 tensor-core path
+// FP16x3 tensor-core path
 // ---------------------------------------------------------------------------
 int64_t tc_rows(int64_t v) { return 128 * round_up(cdiv(v, 128), 2); }
 
@@ -398,13 +398,13 @@ int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
 int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
     CD_RC(require_inputs(ctx, spin));
     SpinState& s = ctx->spin[spin];
-    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_BF16X3)
+    if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_FP16X3)
         return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
     if (!s.B64_valid) {
         CD_RC(transform_f64(ctx, spin));
         s.B16_valid = false;
     }
-    if (precision == MSHQC_CD_BF16X3 && !s.B16_valid) CD_RC(split_fixed(ctx, spin));
+    if (precision == MSHQC_CD_FP16X3 && !s.B16_valid) CD_RC(split_fixed(ctx, spin));
     return MSHQC_CD_OK;
 }
 
@@ -413,7 +413,7 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
     ctx->fixed_point_exact = 1;
     auto pass = [&](int mode, int sx, int sy, double* tot, std::vector<double>& pm,
                     double* tot_os) {
-        return precision == MSHQC_CD_BF16X3 ? pair_pass_tc(ctx, mode, sx, sy, tot, pm, tot_os)
+        return precision == MSHQC_CD_FP16X3 ? pair_pass_tc(ctx, mode, sx, sy, tot, pm, tot_os)
                                             : pair_pass_f64(ctx, mode, sx, sy, tot, pm, tot_os);
     };
     CD_RC(require_inputs(ctx, 0));

@@ -1,5 +1,6 @@
-"""Mixed-precision (BF16x3 on tcgen05, FP32 accumulation, FP64 denominators
-and sums) path vs the FP64 path, the CPU oracle and the reference fixtures.
+"""Mixed-precision path (scaled FP16x3 on tcgen05: exact FP32 accumulation of
+fixed-point products, FP64 denominators and sums) vs the FP64 path, the CPU
+oracle and the reference fixtures.
 
 The mixed path represents every MO row (i,a) in fixed point with one
 power-of-two scale (step 2^-17 of the row maximum) and accumulates the
@@ -46,7 +47,7 @@ def test_restricted_raw_vs_reference(ctx, golden, name):
     g = golden(name)
     o = int(g["nocc"])
     ctx.set_vectors(g["L"]).set_orbitals(capi.ALPHA, g["C"], g["eps"], o)
-    e = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)
+    e = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
     ref = float(g["e_corr"])
     assert abs(e["total"] - ref) <= REL_TOL_RAW_SMALL * abs(ref), (e["total"], ref)
     assert abs(e["os"] - float(g["ump2_os"])) <= REL_TOL_RAW_SMALL * abs(float(g["ump2_os"]))
@@ -56,7 +57,7 @@ def test_restricted_twin_fixture_abs(ctx, golden):
     g = golden("rmp2_twin_n28_o5_m80")
     o = int(g["nocc"])
     ctx.set_vectors(g["L"]).set_orbitals(capi.ALPHA, g["C"], g["eps"], o)
-    e = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)
+    e = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
     assert abs(e["total"] - float(g["e_corr"])) <= ABS_TOL_TWIN
 
 
@@ -66,13 +67,13 @@ def test_restricted_twin_vs_fp64(ctx, N, o, M):
     a = inp.alpha
     ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
     e64 = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)
-    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)
+    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
     assert abs(e3["total"] - e64["total"]) <= ABS_TOL_TWIN, (e3["total"], e64["total"])
     assert abs(e3["os"] - e64["os"]) <= ABS_TOL_TWIN
     # pair energies agree too
     ctx.mp2_energy(capi.RESTRICTED, capi.FP64)
     P64 = ctx.pair_energies(0)
-    ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)
+    ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
     P3 = ctx.pair_energies(0)
     assert np.max(np.abs(P3 - P64)) <= ABS_TOL_TWIN
 
@@ -84,7 +85,7 @@ def test_unrestricted_raw_vs_reference(ctx, golden, name):
     ctx.set_vectors(g["L"])
     ctx.set_orbitals(capi.ALPHA, g["Ca"], g["ea"], na)
     ctx.set_orbitals(capi.BETA, g["Cb"], g["eb"], nb)
-    e = ctx.mp2_energy(capi.UNRESTRICTED, capi.BF16X3)
+    e = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP16X3)
     for k in ("ss_aa", "ss_bb", "os"):
         assert abs(e[k] - float(g[k])) <= REL_TOL_RAW_SMALL * abs(float(g[k])), k
 
@@ -96,7 +97,7 @@ def test_unrestricted_twin_vs_fp64(ctx):
     ctx.set_orbitals(capi.ALPHA, inp.alpha.C, inp.alpha.eps, oa)
     ctx.set_orbitals(capi.BETA, inp.beta.C, inp.beta.eps, ob)
     e64 = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP64)
-    e3 = ctx.mp2_energy(capi.UNRESTRICTED, capi.BF16X3)
+    e3 = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP16X3)
     for k in ("ss_aa", "ss_bb", "os", "total"):
         assert abs(e3[k] - e64[k]) <= ABS_TOL_TWIN, (k, e3[k], e64[k])
 
@@ -106,7 +107,7 @@ def test_mixed_vs_oracle_medium(ctx):
     inp = twin_inputs(N, o, M, seed=12)
     a = inp.alpha
     ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
-    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)
+    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
     B = orc.transform(inp.L, a.C, o)
     E, _ = orc.rmp2_energy(B, a.eps, o)
     assert abs(e3["total"] - E) <= ABS_TOL_TWIN
@@ -118,7 +119,7 @@ def test_restricted_raw_medium_vs_fp64(ctx, N, o, M):
     a = inp.alpha
     ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
     e64 = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)["total"]
-    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)["total"]
+    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)["total"]
     assert abs(e3 - e64) <= REL_TOL_RAW * abs(e64), (e3, e64)
 
 
@@ -126,7 +127,7 @@ def test_mixed_deterministic(ctx, golden):
     g = golden("rmp2_n32_o6_m96")
     o = int(g["nocc"])
     ctx.set_vectors(g["L"]).set_orbitals(capi.ALPHA, g["C"], g["eps"], o)
-    e1 = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)["total"]
+    e1 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)["total"]
     ctx.set_orbitals(capi.ALPHA, g["C"], g["eps"], o)
-    e2 = ctx.mp2_energy(capi.RESTRICTED, capi.BF16X3)["total"]
+    e2 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)["total"]
     assert e1 == e2
