@@ -382,6 +382,7 @@ int mshqc_cd_set_orbitals(mshqc_cd_ctx* ctx, int spin, const double* C, const do
     s.set = true;
     s.invalidate();
     ctx->diag_os_valid = false;
+    if (ctx->Y_spin == spin) ctx->Y_spin = -1;
     CD_CUDA(cudaStreamSynchronize(ctx->stream));
     return MSHQC_CD_OK;
 }

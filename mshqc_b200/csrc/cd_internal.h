@@ -69,6 +69,7 @@ struct mshqc_cd_ctx {
 
     // workspaces
     mshqc_cd::DevBuf Y;             // half-transformed vectors
+    int Y_spin = -1;                // spin whose Y is in the buffer (-1: none)
     mshqc_cd::DevBuf scratch;       // uploads / unpacking
     mshqc_cd::DevBuf tables;        // pair and block tables
     mshqc_cd::DevBuf partial;       // per-unit energies
@@ -90,6 +91,7 @@ struct mshqc_cd_ctx {
         spin[0].invalidate();
         spin[1].invalidate();
         diag_os_valid = false;
+        Y_spin = -1;
         for (auto& p : pair_energy) p.clear();
     }
     size_t held_bytes() const {

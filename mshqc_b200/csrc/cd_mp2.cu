@@ -14,6 +14,7 @@
 #include "pair_energy_f64.cuh"
 #include "pair_energy_tc.cuh"
 #include "split_bf16.cuh"
+#include "backward_f64.cuh"
 
 namespace mshqc_cd {
 
@@ -81,6 +82,7 @@ int transform_f64(mshqc_cd_ctx* ctx, int spin) {
     CD_CUDA(gemm_f64(g2, true, true, ctx->stream));
     ctx->launches++;
     s.B64_valid = true;
+    ctx->Y_spin = spin;
     return MSHQC_CD_OK;
 }
 
@@ -451,11 +453,144 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
     return MSHQC_CD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// backward
+// ---------------------------------------------------------------------------
+namespace {
+
+// Restricted FP64 gradient: amplitude pass + Gamma GEMM per block of occupied
+// rows, then the transposed half transforms.  dC (column-major N*N, device),
+// deps (N, device) are written; *energy gets the closed-shell E.
+int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
+    SpinState& s = ctx->spin[0];
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
+    const int nb = (int)(vp / 64);
+    // occupied block size for the amplitude staging buffer
+    size_t free_b = 0, total_b = 0;
+    CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_i = sizeof(double) * (size_t)vp * o * vp;
+    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 4, size_t(16) << 30));
+    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(budget / per_i)));
+    CD_ALLOC(ctx->amp, per_i * bi, false);
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, false);
+    CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
+    const int64_t units_per_i = (int64_t)o * nb * nb;
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), false);
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+    const size_t smem = pair_f64_detail::SMEM_BYTES;
+    CD_CUDA(cudaFuncSetAttribute(amp_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int i0 = 0; i0 < o; i0 += bi) {
+        const int nbi = (int)std::min<int64_t>(bi, o - i0);
+        AmpF64Args a{};
+        a.X = s.B64.as<double>();
+        a.o = (int)o;  a.v = (int)v;  a.vp = (int)vp;  a.Mp = (int)Mp;
+        a.i0 = i0;  a.bi = nbi;
+        a.eo = s.eps.as<double>();  a.ev = a.eo + o;
+        a.amp = ctx->amp.as<double>();
+        a.deps = deps;
+        a.partial = ctx->partial.as<double>() + (int64_t)i0 * units_per_i;
+        a.nb = nb;
+        const int64_t units = (int64_t)nbi * units_per_i;
+        amp_f64_kernel<<<(unsigned)units, 256, smem, ctx->stream>>>(a);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+        // Gamma[(i,a)][Q] = sum_{(j,b)} tt[(i,a)][(j,b)] B[(j,b)][Q]
+        GemmF64Args g{};
+        g.M = (int)(nbi * vp);  g.N = (int)Mp;  g.K = (int)(o * vp);  g.batch = 1;
+        g.A = ctx->amp.as<double>();  g.lda = o * vp;  g.sA = 0;
+        g.B = s.B64.as<double>();  g.ldb = Mp;  g.sB = 0;
+        g.C = ctx->gam[0].as<double>() + (int64_t)i0 * vp * Mp;  g.ldc = Mp;  g.sC = 0;
+        g.alpha = 1.0;  g.beta = 0.0;
+        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+    }
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * units_per_i),
+                                                   ctx->totals.as<double>());
+    CD_CUDA(cudaGetLastError());
+    ctx->launches++;
+    CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+
+    // dE/dB = 4 Gamma.  Y[i][Q][nu] (half-transformed vectors) is needed.
+    if (ctx->Y_spin != 0) {
+        s.B64_valid = false;
+        CD_RC(transform_f64(ctx, 0));
+    }
+    const double* C = s.C.as<double>();
+    const double* Gm = ctx->gam[0].as<double>();
+    // dC[nu, o+a] = 4 sum_{i,Q} Gamma[i][a][Q] Y[i][Q][nu]   (row-major [a][nu] == column-major dC)
+    for (int64_t i = 0; i < o; ++i) {
+        GemmF64Args g{};
+        g.M = (int)v;  g.N = (int)N;  g.K = (int)M;  g.batch = 1;
+        g.A = Gm + i * vp * Mp;  g.lda = Mp;  g.sA = 0;
+        g.B = ctx->Y.as<double>() + i * M * N;  g.ldb = N;  g.sB = 0;
+        g.C = dC + o * N;  g.ldc = N;  g.sC = 0;
+        g.alpha = 4.0;  g.beta = i == 0 ? 0.0 : 1.0;
+        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+    }
+    // W[i][Q][nu] = sum_a Gamma[i][a][Q] C[nu, o+a]   (into the Y buffer)
+    {
+        GemmF64Args g{};
+        g.M = (int)M;  g.N = (int)N;  g.K = (int)v;  g.batch = (int)o;
+        g.A = Gm;  g.lda = Mp;  g.sA = vp * Mp;
+        g.B = C + o * N;  g.ldb = N;  g.sB = 0;
+        g.C = ctx->Y.as<double>();  g.ldc = N;  g.sC = M * N;
+        g.alpha = 1.0;  g.beta = 0.0;
+        CD_CUDA(gemm_f64(g, false, false, ctx->stream));
+        ctx->launches++;
+        ctx->Y_spin = -1;
+    }
+    // dC[mu, i] = 4 sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]
+    {
+        GemmF64Args g{};
+        g.M = (int)o;  g.N = (int)N;  g.K = (int)(M * N);  g.batch = 1;
+        g.A = ctx->Y.as<double>();  g.lda = M * N;  g.sA = 0;
+        g.B = ctx->L.as<double>();  g.ldb = N;  g.sB = 0;
+        g.C = dC;  g.ldc = N;  g.sC = 0;
+        g.alpha = 4.0;  g.beta = 0.0;
+        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+    }
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MSHQC_CD_OK;
+}
+
+}  // namespace
+
 int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out, double* dC_a,
                  double* dC_b, double* deps_a, double* deps_b, int where) {
-    (void)ctx; (void)kind; (void)precision; (void)e_out; (void)dC_a; (void)dC_b;
-    (void)deps_a; (void)deps_b; (void)where;
-    return set_error(MSHQC_CD_ERR_UNSUPPORTED, "gradient path not built yet");
+    if (kind != MSHQC_CD_RESTRICTED)
+        return set_error(MSHQC_CD_ERR_UNSUPPORTED, "unrestricted gradient not built yet");
+    if (precision != MSHQC_CD_FP64)
+        return set_error(MSHQC_CD_ERR_UNSUPPORTED, "mixed-precision gradient not built yet");
+    (void)dC_b;
+    (void)deps_b;
+    CD_RC(require_inputs(ctx, 0));
+    const int64_t N = ctx->N;
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    CD_CUDA(cudaEventRecord(e0, ctx->stream));
+    CD_RC(ensure_transform(ctx, 0, MSHQC_CD_FP64));
+    CD_CUDA(cudaEventRecord(e1, ctx->stream));
+    CD_ALLOC(ctx->grad[0], sizeof(double) * (size_t)(N * N + N), false);
+    double* dC = ctx->grad[0].as<double>();
+    double* de = dC + N * N;
+    double energy = 0.0;
+    CD_RC(gradient_restricted_f64(ctx, dC, de, &energy));
+    CD_CUDA(cudaEventRecord(e2, ctx->stream));
+    CD_CUDA(cudaEventSynchronize(e2));
+    if (e_out) {
+        std::memset(e_out, 0, sizeof(*e_out));
+        e_out->total = energy;
+        float t01 = 0, t12 = 0;
+        CD_CUDA(cudaEventElapsedTime(&t01, e0, e1));
+        CD_CUDA(cudaEventElapsedTime(&t12, e1, e2));
+        e_out->ms_transform = t01;
+        e_out->ms_energy = t12;
+        e_out->ms_total = t01 + t12;
+    }
+    CD_RC(download(ctx, dC_a, dC, sizeof(double) * N * N, where));
+    CD_RC(download(ctx, deps_a, de, sizeof(double) * N, where));
+    return MSHQC_CD_OK;
 }
 
 }  // namespace mshqc_cd
