@@ -78,7 +78,8 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf flag;          // error / NaN flags
     mshqc_cd::DevBuf amp;           // backward: staged amplitudes
     mshqc_cd::DevBuf gam[2];        // backward: Gamma per spin
-    mshqc_cd::DevBuf BT;            // backward: transposed MO vectors
+    mshqc_cd::DevBuf BT;            // backward: transposed MO vectors (hi/lo BF16)
+    mshqc_cd::DevBuf amp2;          // backward: second half of the staging (lo)
     mshqc_cd::DevBuf W;             // backward: C_vir-contracted Gamma
     mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
     mshqc_cd::DevBuf diag_os;       // sum_Q B_alpha[i][a] B_beta[i][a] (opposite-spin diagonal)
@@ -96,7 +97,7 @@ struct mshqc_cd_ctx {
     }
     size_t held_bytes() const {
         size_t b = L.bytes + Y.bytes + scratch.bytes + tables.bytes + partial.bytes +
-                   pair_sum.bytes + totals.bytes + flag.bytes + amp.bytes + BT.bytes + W.bytes;
+                   pair_sum.bytes + totals.bytes + flag.bytes + amp.bytes + amp2.bytes + BT.bytes + W.bytes;
         for (const auto& s : spin)
             b += s.C.bytes + s.eps.bytes + s.B64.bytes + s.Bhi.bytes + s.Blo.bytes + s.expo.bytes +
                  s.diag.bytes + s.norms.bytes;
@@ -116,6 +117,7 @@ struct mshqc_cd_ctx {
         flag.release();
         amp.release();
         BT.release();
+        amp2.release();
         W.release();
         for (auto& s : spin) {
             s.C.release();

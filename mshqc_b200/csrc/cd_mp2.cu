@@ -15,6 +15,7 @@
 #include "pair_energy_tc.cuh"
 #include "split_bf16.cuh"
 #include "backward_f64.cuh"
+#include "gamma_tc.cuh"
 
 namespace mshqc_cd {
 
@@ -306,6 +307,15 @@ UnitTables make_tables_tc(int mode, int ox, int oy, int nbx, int nby) {
     return t;
 }
 
+UnitTables make_tables_amp(int i0, int nbi, int o, int nb) {
+    UnitTables t;
+    for (int i = i0; i < i0 + nbi; ++i)
+        for (int j = 0; j < o; ++j) t.pairs.push_back(make_int2(i, j));
+    for (int x = 0; x < nb; ++x)
+        for (int y = 0; y < nb; ++y) t.blocks.push_back(make_int2(x, y));
+    return t;
+}
+
 template <int MODE>
 cudaError_t launch_tc(const PairTcArgs& a, int grid, cudaStream_t st) {
     const size_t smem = pair_tc::SMEM_BYTES;
@@ -458,6 +468,56 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
 // ---------------------------------------------------------------------------
 namespace {
 
+// dE/dC from Gamma (in ctx->gam[0], [o][vp][Mp] FP64): dE/dB = 4 Gamma,
+// dC[nu, o+a] = sum_{i,Q} dE/dB[i][a][Q] Y[i][Q][nu],
+// dC[mu, i]   = sum_{Q,nu} L[Q][nu][mu] sum_a dE/dB[i][a][Q] C[nu, o+a].
+int transposed_transforms(mshqc_cd_ctx* ctx, double* dC) {
+    SpinState& s = ctx->spin[0];
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
+    // dE/dB = 4 Gamma.  Y[i][Q][nu] (half-transformed vectors) is needed.
+    if (ctx->Y_spin != 0) {
+        s.B64_valid = false;
+        CD_RC(transform_f64(ctx, 0));
+    }
+    const double* C = s.C.as<double>();
+    const double* Gm = ctx->gam[0].as<double>();
+    // dC[nu, o+a] = 4 sum_{i,Q} Gamma[i][a][Q] Y[i][Q][nu]   (row-major [a][nu] == column-major dC)
+    for (int64_t i = 0; i < o; ++i) {
+        GemmF64Args g{};
+        g.M = (int)v;  g.N = (int)N;  g.K = (int)M;  g.batch = 1;
+        g.A = Gm + i * vp * Mp;  g.lda = Mp;  g.sA = 0;
+        g.B = ctx->Y.as<double>() + i * M * N;  g.ldb = N;  g.sB = 0;
+        g.C = dC + o * N;  g.ldc = N;  g.sC = 0;
+        g.alpha = 4.0;  g.beta = i == 0 ? 0.0 : 1.0;
+        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+    }
+    // W[i][Q][nu] = sum_a Gamma[i][a][Q] C[nu, o+a]   (into the Y buffer)
+    {
+        GemmF64Args g{};
+        g.M = (int)M;  g.N = (int)N;  g.K = (int)v;  g.batch = (int)o;
+        g.A = Gm;  g.lda = Mp;  g.sA = vp * Mp;
+        g.B = C + o * N;  g.ldb = N;  g.sB = 0;
+        g.C = ctx->Y.as<double>();  g.ldc = N;  g.sC = M * N;
+        g.alpha = 1.0;  g.beta = 0.0;
+        CD_CUDA(gemm_f64(g, false, false, ctx->stream));
+        ctx->launches++;
+        ctx->Y_spin = -1;
+    }
+    // dC[mu, i] = 4 sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]
+    {
+        GemmF64Args g{};
+        g.M = (int)o;  g.N = (int)N;  g.K = (int)(M * N);  g.batch = 1;
+        g.A = ctx->Y.as<double>();  g.lda = M * N;  g.sA = 0;
+        g.B = ctx->L.as<double>();  g.ldb = N;  g.sB = 0;
+        g.C = dC;  g.ldc = N;  g.sC = 0;
+        g.alpha = 4.0;  g.beta = 0.0;
+        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+    }
+    return MSHQC_CD_OK;
+}
+
 // Restricted FP64 gradient: amplitude pass + Gamma GEMM per block of occupied
 // rows, then the transposed half transforms.  dC (column-major N*N, device),
 // deps (N, device) are written; *energy gets the closed-shell E.
@@ -510,48 +570,115 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
     ctx->launches++;
     CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 
-    // dE/dB = 4 Gamma.  Y[i][Q][nu] (half-transformed vectors) is needed.
-    if (ctx->Y_spin != 0) {
-        s.B64_valid = false;
-        CD_RC(transform_f64(ctx, 0));
-    }
-    const double* C = s.C.as<double>();
-    const double* Gm = ctx->gam[0].as<double>();
-    // dC[nu, o+a] = 4 sum_{i,Q} Gamma[i][a][Q] Y[i][Q][nu]   (row-major [a][nu] == column-major dC)
-    for (int64_t i = 0; i < o; ++i) {
-        GemmF64Args g{};
-        g.M = (int)v;  g.N = (int)N;  g.K = (int)M;  g.batch = 1;
-        g.A = Gm + i * vp * Mp;  g.lda = Mp;  g.sA = 0;
-        g.B = ctx->Y.as<double>() + i * M * N;  g.ldb = N;  g.sB = 0;
-        g.C = dC + o * N;  g.ldc = N;  g.sC = 0;
-        g.alpha = 4.0;  g.beta = i == 0 ? 0.0 : 1.0;
-        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
-        ctx->launches++;
-    }
-    // W[i][Q][nu] = sum_a Gamma[i][a][Q] C[nu, o+a]   (into the Y buffer)
-    {
-        GemmF64Args g{};
-        g.M = (int)M;  g.N = (int)N;  g.K = (int)v;  g.batch = (int)o;
-        g.A = Gm;  g.lda = Mp;  g.sA = vp * Mp;
-        g.B = C + o * N;  g.ldb = N;  g.sB = 0;
-        g.C = ctx->Y.as<double>();  g.ldc = N;  g.sC = M * N;
-        g.alpha = 1.0;  g.beta = 0.0;
-        CD_CUDA(gemm_f64(g, false, false, ctx->stream));
-        ctx->launches++;
-        ctx->Y_spin = -1;
-    }
-    // dC[mu, i] = 4 sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]
-    {
-        GemmF64Args g{};
-        g.M = (int)o;  g.N = (int)N;  g.K = (int)(M * N);  g.batch = 1;
-        g.A = ctx->Y.as<double>();  g.lda = M * N;  g.sA = 0;
-        g.B = ctx->L.as<double>();  g.ldb = N;  g.sB = 0;
-        g.C = dC;  g.ldc = N;  g.sC = 0;
-        g.alpha = 4.0;  g.beta = 0.0;
-        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
-        ctx->launches++;
-    }
+    CD_RC(transposed_transforms(ctx, dC));
     CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MSHQC_CD_OK;
+}
+
+
+// Restricted mixed-precision gradient: exact fixed-point amplitude pass on
+// the tensor cores (writes tt as BF16 hi/lo), tensor-core Gamma GEMM with
+// round-to-nearest promotion, then the FP64 transposed transforms.
+int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
+    SpinState& s = ctx->spin[0];
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
+    const int64_t nblk = cdiv(v, 128), VR = nblk * 128, RQ = round_up(M, 256);
+    const int64_t KA = o * VR;
+    // transposed hi/lo copy of B: rows Q, K = (j, b)
+    const size_t nbt = (size_t)RQ * KA;
+    CD_ALLOC(ctx->BT, 2 * nbt * sizeof(uint16_t), false);
+    uint16_t* bth = ctx->BT.as<uint16_t>();
+    uint16_t* btl = bth + nbt;
+    {
+        const int64_t threads = (KA / 16) * RQ * 2;
+        const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
+        bt_split_kernel<<<blocks, 256, 0, ctx->stream>>>(s.B64.as<double>(), vp, Mp, (int)v, (int)M, o,
+                                                         VR, RQ, bth, btl);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+    }
+    // occupied block size for the staging (2 x BF16 per element)
+    size_t free_b = 0, total_b = 0;
+    CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_i = sizeof(uint16_t) * (size_t)VR * KA;
+    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 6, size_t(24) << 30));
+    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(budget / per_i)));
+    CD_ALLOC(ctx->amp, per_i * bi, false);
+    CD_ALLOC(ctx->amp2, per_i * bi, false);
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, true);
+    CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
+    CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+    const int64_t units_per_i = o * nblk * nblk;
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), false);
+    for (int i0 = 0; i0 < o; i0 += bi) {
+        const int nbi = (int)std::min<int64_t>(bi, o - i0);
+        UnitTables t = make_tables_amp(i0, nbi, (int)o, (int)nblk);
+        const int npairs = (int)t.pairs.size(), nblocks = (int)t.blocks.size();
+        CD_ALLOC(ctx->tables, sizeof(int2) * (t.pairs.size() + t.blocks.size()), false);
+        int2* dpairs = ctx->tables.as<int2>();
+        CD_CUDA(cudaMemcpyAsync(dpairs, t.pairs.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        CD_CUDA(cudaMemcpyAsync(dpairs + npairs, t.blocks.data(), sizeof(int2) * nblocks,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        const int64_t units = (int64_t)npairs * nblocks;
+        PairTcArgs a{};
+        a.Xhi = s.Bhi.as<uint16_t>();  a.Xlo = s.Blo.as<uint16_t>();
+        a.Yhi = a.Xhi;  a.Ylo = a.Xlo;
+        a.ex = s.expo.as<int>();  a.ey = a.ex;
+        a.diag = s.diag.as<double>();
+        a.rows_x = a.rows_y = (int)s.vp16;
+        a.nqc = (int)(Mp / 16);
+        a.vx = a.vy = (int)v;
+        a.diag_o = (int)o;  a.diag_v = (int)v;
+        a.eox = s.eps.as<double>();  a.evx = a.eox + o;
+        a.eoy = a.eox;  a.evy = a.evx;
+        a.pairs = dpairs;  a.blocks = dpairs + npairs;  a.nblocks = nblocks;
+        a.units = units;
+        a.partial = ctx->partial.as<double>() + (int64_t)i0 * units_per_i;
+        a.partial2 = nullptr;
+        a.err = ctx->flag.as<int>();
+        a.amp_hi = ctx->amp.as<uint16_t>();
+        a.amp_lo = ctx->amp2.as<uint16_t>();
+        a.amp_rows = (long long)bi * VR;
+        a.VR = (int)VR;
+        a.i0 = i0;
+        a.deps = deps;
+        const int grid = (int)std::min<int64_t>(units, ctx->num_sms);
+        cudaError_t e = launch_tc<PAIR_AMPLITUDE>(a, grid, ctx->stream);
+        if (e != cudaSuccess) return cuda_error(e, "amplitude kernel launch");
+        ctx->launches++;
+        GammaTcArgs g{};
+        g.Ahi = ctx->amp.as<uint16_t>();  g.Alo = ctx->amp2.as<uint16_t>();
+        g.Bhi = bth;  g.Blo = btl;
+        g.RA = (long long)bi * VR;  g.RQ = RQ;
+        g.nk = (int)(KA / 16);
+        g.KP = 32;
+        g.nrb = (int)(nbi * VR / 128);
+        g.nqb = (int)(RQ / 256);
+        g.VR = (int)VR;  g.v = (int)v;  g.vp = (int)vp;  g.Mp = (int)Mp;  g.i0 = i0;
+        g.gamma = ctx->gam[0].as<double>();
+        g.err = ctx->flag.as<int>() + 2;
+        const size_t gsm = gamma_tc::SMEM_BYTES;
+        CD_CUDA(cudaFuncSetAttribute(gamma_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+        const int ggrid = (int)std::min<int64_t>((int64_t)g.nrb * g.nqb, ctx->num_sms);
+        gamma_tc_kernel<<<ggrid, gamma_tc::THREADS, gsm, ctx->stream>>>(g);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+    }
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * units_per_i),
+                                                   ctx->totals.as<double>());
+    CD_CUDA(cudaGetLastError());
+    ctx->launches++;
+    int herr[4] = {0, 0, 0, 0};
+    CD_CUDA(cudaMemcpyAsync(herr, ctx->flag.p, sizeof(herr), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (herr[0] || herr[2])
+        return set_error(MSHQC_CD_ERR_TIMEOUT, "tensor-core backward gave up waiting (site " +
+                                                   std::to_string(herr[0] ? herr[0] : herr[2]) + ")");
+    if (herr[1]) ctx->fixed_point_exact = 0;
+    CD_RC(transposed_transforms(ctx, dC));
     return MSHQC_CD_OK;
 }
 
@@ -561,21 +688,23 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
                  double* dC_b, double* deps_a, double* deps_b, int where) {
     if (kind != MSHQC_CD_RESTRICTED)
         return set_error(MSHQC_CD_ERR_UNSUPPORTED, "unrestricted gradient not built yet");
-    if (precision != MSHQC_CD_FP64)
-        return set_error(MSHQC_CD_ERR_UNSUPPORTED, "mixed-precision gradient not built yet");
     (void)dC_b;
     (void)deps_b;
     CD_RC(require_inputs(ctx, 0));
     const int64_t N = ctx->N;
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     CD_CUDA(cudaEventRecord(e0, ctx->stream));
-    CD_RC(ensure_transform(ctx, 0, MSHQC_CD_FP64));
+    CD_RC(ensure_transform(ctx, 0, precision));
     CD_CUDA(cudaEventRecord(e1, ctx->stream));
     CD_ALLOC(ctx->grad[0], sizeof(double) * (size_t)(N * N + N), false);
     double* dC = ctx->grad[0].as<double>();
     double* de = dC + N * N;
     double energy = 0.0;
-    CD_RC(gradient_restricted_f64(ctx, dC, de, &energy));
+    ctx->fixed_point_exact = 1;
+    if (precision == MSHQC_CD_FP64)
+        CD_RC(gradient_restricted_f64(ctx, dC, de, &energy));
+    else
+        CD_RC(gradient_restricted_tc(ctx, dC, de, &energy));
     CD_CUDA(cudaEventRecord(e2, ctx->stream));
     CD_CUDA(cudaEventSynchronize(e2));
     if (e_out) {

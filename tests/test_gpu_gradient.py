@@ -58,3 +58,31 @@ def test_restricted_fp64_orbital_gradient_fd(ctx):
         em = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)["total"]
         fd = (ep - em) / (2 * h)
         assert abs(fd - kg[ai, ii]) <= 1e-6, (ai, ii, fd, kg[ai, ii])
+
+
+# Mixed precision: the same derivatives from the tensor-core path (exact
+# fixed-point amplitude pass, Gamma GEMM with round-to-nearest promotion).
+# Tolerance on scaled-twin inputs: max |d dE/dC|, max |d dE/deps| <= 1e-6,
+# energy <= 1 micro-Eh.
+@pytest.mark.parametrize("N,o,M,seed", [(60, 8, 150, 3), (131, 14, 300, 5), (257, 21, 640, 6)])
+def test_restricted_mixed_gradient_vs_fp64(ctx, N, o, M, seed):
+    inp = twin(N, o, M, seed=seed)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    g64 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
+    g3 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
+    assert abs(g3.energy["total"] - g64.energy["total"]) <= 1e-6
+    assert np.max(np.abs(g3.dC_a - g64.dC_a)) <= 1e-6, np.max(np.abs(g3.dC_a - g64.dC_a))
+    assert np.max(np.abs(g3.deps_a - g64.deps_a)) <= 1e-6, np.max(np.abs(g3.deps_a - g64.deps_a))
+
+
+def test_restricted_mixed_gradient_vs_oracle(ctx):
+    N, o, M = 48, 6, 120
+    inp = twin(N, o, M, seed=8)
+    a = inp.alpha
+    ref = orc.restricted_gradient(inp.L, a.C, a.eps, o)
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    g = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
+    assert abs(g.energy["total"] - ref["E"]) <= 1e-6
+    assert np.max(np.abs(g.dC_a - ref["dC"])) <= 1e-6
+    assert np.max(np.abs(g.deps_a - ref["deps"])) <= 1e-6
