@@ -4,19 +4,28 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
     python bench.py --impl reference ...   # the reference CPU path
 
-One step = one pass of the hot path over one synthetic input (seeded recipe
-of mshqc_b200/synthetic.py): AO->MO half transforms plus the fused pair
-kernels (plus the backward for gradient workloads).  `value` is FP64-
-equivalent algorithmic TFLOP/s over all ranks with the inputs resident in
-HBM; `e2e` is the same metric through the C ABI from pinned host buffers,
-host<->device copies inside the timed region.  Multi-GPU runs are replicas
+Default workload: CD-MP2 energy plus the exact orbital gradient (dE/dC,
+dE/deps) of a closed-shell system with N=1000 basis functions, o=100
+occupied orbitals and M=4000 Cholesky vectors (the largest of the synthetic
+configurations whose FP64 AO vectors fit one GPU; the N=2000 one needs 256 GB
+of AO vectors), synthetic inputs of the seeded recipe in
+mshqc_b200/synthetic.py at the scaled magnitude |E_corr| ~ 0.05 o Eh.
+
+One step = AO->MO half transform + fused amplitude/energy pass + Gamma GEMM +
+transposed transforms, i.e. one mp2_gradient call, in the mixed precision
+(scaled FP16x3 on the tensor cores).  The FP64 path is timed on the same
+inputs for the mixed-vs-FP64 comparison and the energy / gradient errors.
+
+`value` = FP64-equivalent algorithmic TFLOP/s over all ranks with the inputs
+resident in HBM (work 2 F_T + 2 F_E + 2 v^2 M o^2; F_T = 2 M N o (N+v),
+F_E = v^2 M o (o+1)); `e2e` = the same metric through the C ABI from pinned
+host buffers, copies inside the timed region.  Multi-GPU runs are replicas
 (independent inputs per rank, weak scaling, no data-path collective).
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -29,14 +38,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# workload name -> (N, o, M, kind, precision, gradient)
+METRIC = "CD-MP2 energy+OMP2 grad s & TFLOP/s: mixed vs FP64 on B200 at ≤1 µEh"
+
 WORKLOADS = {
-    "cdrmp2_fp64_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
-                                       precision="fp64", gradient=False),
-    "cdrmp2_fp16x3_n400_o40_m1600": dict(N=400, o=40, M=1600, kind="restricted",
-                                         precision="fp16x3", gradient=False),
+    # headline: energy + exact gradient, mixed vs FP64
+    "cdmp2_grad_n1000_o100_m4000": dict(N=1000, o=100, M=4000, gradient=True, precision="fp16x3"),
+    # smaller variant of the same step
+    "cdmp2_grad_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=True, precision="fp16x3"),
+    # energy only (the CD-RMP2 drop-in), N=400, o=40, M=1600
+    "cdrmp2_energy_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=False, precision="fp16x3"),
 }
-DEFAULT_WORKLOAD = "cdrmp2_fp64_n400_o40_m1600"
+DEFAULT_WORKLOAD = "cdmp2_grad_n1000_o100_m4000"
 
 
 # ---------------------------------------------------------------------------
@@ -46,19 +58,20 @@ def flops_transform(N, o, M):
     return 2.0 * M * N * o * (N + (N - o))
 
 
-def flops_energy(N, o, M, restricted=True, ob=None):
+def flops_energy(N, o, M):
     v = N - o
-    if restricted:
-        pairs = o * (o + 1) / 2
-        return 2.0 * v * v * M * pairs
-    vb = N - ob
-    return 2.0 * M * (v * v * o * (o - 1) / 2 + vb * vb * ob * (ob - 1) / 2 + v * vb * o * ob)
+    return 1.0 * v * v * M * o * (o + 1)
 
 
-def workload_flops(w):
-    N, o, M = w["N"], w["o"], w["M"]
-    f = flops_transform(N, o, M) + flops_energy(N, o, M)
-    return f
+def flops_gamma(N, o, M):
+    v = N - o
+    return 2.0 * v * v * M * o * o
+
+
+def workload_flops(N, o, M, gradient):
+    if not gradient:
+        return flops_transform(N, o, M) + flops_energy(N, o, M)
+    return 2 * flops_transform(N, o, M) + 2 * flops_energy(N, o, M) + flops_gamma(N, o, M)
 
 
 # ---------------------------------------------------------------------------
@@ -74,6 +87,8 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self._t = None
+        self.t_begin = 0.0
+        self.t_end = float("inf")
 
     def start(self):
         try:
@@ -91,9 +106,6 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append((time.time(), line.strip()))
 
-    def mark(self, name):
-        setattr(self, name, time.time())
-
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -104,13 +116,9 @@ class ClockSampler:
             self.proc.kill()
         if self._t:
             self._t.join(timeout=2)
-        sm, smax, reasons = [], None, set()
+        sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        # samples inside the timed window (widened by one sampling period on
-        # each side so that short windows still get the neighbouring samples)
-        t0 = getattr(self, "t_begin", 0.0) - 0.25
-        t1 = getattr(self, "t_end", float("inf")) + 0.25
-        window = [ln for (t, ln) in self.lines if t0 <= t <= t1]
+        window = [ln for (t, ln) in self.lines if self.t_begin - 0.25 <= t <= self.t_end + 0.25]
         for ln in window:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -118,27 +126,27 @@ class ClockSampler:
             try:
                 sm.append(float(parts[1]))
                 smax = float(parts[2])
+                power.append(float(parts[3]))
             except ValueError:
                 continue
             for name, val in zip(names, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
 
 
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         with open(path) as f:
-            d = json.load(f)
-        return d, "measured"
+            return json.load(f), "measured"
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
 def measure_fp64_peak(torch, device):
-    """cuBLAS FP64 GEMM throughput (torch float64 matmul 8192^3, best of 5):
-    the denominator of the FP64 roofline (MEASURED_PEAKS.json has none)."""
+    """cuBLAS FP64 GEMM rate (torch float64 matmul 8192^3, best of 5)."""
     n = 8192
     a = torch.randn(n, n, dtype=torch.float64, device=device)
     b = torch.randn(n, n, dtype=torch.float64, device=device)
@@ -160,23 +168,30 @@ def measure_fp64_peak(torch, device):
 # ---------------------------------------------------------------------------
 # reference CPU path (oracle/_ref: the reference's own code, compiled here)
 # ---------------------------------------------------------------------------
-def reference_sample(w, seed=0):
-    """A bounded sample of the workload for the reference CPU path: same N
-    and M, fewer occupied orbitals, so one run takes seconds."""
-    N, o, M = w["N"], w["o"], w["M"]
-    o_s = max(2, min(o, int(os.environ.get("MSHQC_REF_SAMPLE_OCC", "12"))))
-    return N, o_s, M
+REF_SAMPLE = dict(N=300, o=10, M=1200)
 
 
 def run_reference_once(w, seed, nthreads):
+    """One bounded sample of the workload on the reference's own CPU code:
+    CholeskyOMP2's energy + orbital-gradient evaluation (t2, E, OPDM,
+    generalized Fock, w_ai; src/mp2/cholesky_omp2.cc:441-466) for gradient
+    workloads, CholeskyRMP2::compute for energy workloads."""
     from mshqc_b200 import synthetic as syn
     from oracle import ref
-    N, o_s, M = reference_sample(w, seed)
-    inp = syn.make_inputs(N, o_s, M, seed=seed)
+    N, o, M = REF_SAMPLE["N"], REF_SAMPLE["o"], REF_SAMPLE["M"]
+    base = syn.make_inputs(N, o, M, seed=seed)
+    sig = syn.twin_sigma(N, o, M, base.alpha.eps)
+    inp = syn.make_inputs(N, o, M, seed=seed, sigma=sig)
     a = inp.alpha
-    r = ref.rmp2(inp.L, a.C, a.eps, o_s, nthreads=nthreads)
-    flops = flops_transform(N, o_s, M) + flops_energy(N, o_s, M)
-    return r["seconds"], flops, f"N={N}, o={o_s}, M={M} CD-RMP2 (reference CholeskyRMP2::compute)"
+    if w["gradient"]:
+        H = np.eye(N)   # the cost of the Fock build does not depend on H
+        r = ref.omp2_pieces(inp.L, a.C, a.C, a.eps, a.eps, o, o, H, nthreads=nthreads)
+        what = "CholeskyOMP2 energy + w_ai"
+    else:
+        r = ref.rmp2(inp.L, a.C, a.eps, o, nthreads=nthreads)
+        what = "CholeskyRMP2::compute"
+    flops = workload_flops(N, o, M, w["gradient"])
+    return r["seconds"], flops, f"N={N}, o={o}, M={M} {what}"
 
 
 def bench_reference(args, w, rank, world):
@@ -196,8 +211,8 @@ def bench_reference(args, w, rank, world):
         flops = f
     tot = sum(times)
     value = flops * args.steps / tot / 1e12
-    line = {
-        "impl": "reference", "metric": metric_name(w), "value": value, "unit": "TFLOP/s",
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -206,12 +221,7 @@ def bench_reference(args, w, rank, world):
                          "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line))
-
-
-def metric_name(w):
-    return "CD-MP2 energy+OMP2 grad s & TFLOP/s: mixed vs FP64 on B200 at ≤1 µEh"
+    }))
 
 
 # ---------------------------------------------------------------------------
@@ -226,136 +236,175 @@ def bench_gpu(args, w, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     N, o, M = w["N"], w["o"], w["M"]
+    gradient = w["gradient"]
     prec = capi.PRECISIONS[w["precision"]]
-    kind = capi.RESTRICTED if w["kind"] == "restricted" else capi.UNRESTRICTED
+    seed = 1000 + rank
 
-    inp = syn.make_inputs(N, o, M, seed=1000 + rank)
-    a = inp.alpha
-    # pinned host copies for the end-to-end leg
-    L_host = torch.from_numpy(inp.L).pin_memory()
-    C_host = torch.from_numpy(np.asfortranarray(a.C)).pin_memory()
-    e_host = torch.from_numpy(a.eps.copy()).pin_memory()
-    # device-resident inputs for the kernel leg
-    L_dev = L_host.to(dev)
-    C_dev = torch.from_numpy(a.C).to(dev)
-    e_dev = torch.from_numpy(a.eps).to(dev)
+    orb = syn.make_orbitals(N, o, seed)
+    sigma = syn.twin_sigma(N, o, M, orb.eps)
+    L_dev = syn.make_vectors_device(N, M, seed, sigma, dev)
+    C_dev = torch.from_numpy(orb.C).to(dev)
+    e_dev = torch.from_numpy(orb.eps).to(dev)
 
     stream = torch.cuda.Stream(device=dev)
     ctx = capi.Context(local_rank)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_vectors(L_dev)
 
-    def step_device():
-        ctx.set_orbitals(capi.ALPHA, C_dev, e_dev, o)     # new orbitals: full recompute
-        return ctx.mp2_energy(kind, prec)
+    def step(context, precision, C, eps):
+        context.set_orbitals(capi.ALPHA, C, eps, o)            # new orbitals: full recompute
+        if gradient:
+            return context.mp2_gradient(capi.RESTRICTED, precision)
+        return context.mp2_energy(capi.RESTRICTED, precision)
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    for _ in range(max(3, args.warmup)):
-        step_device()
+    for _ in range(args.warmup):
+        r = step(ctx, prec, C_dev, e_dev)
     torch.cuda.synchronize()
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-    time.sleep(1.0)                      # nvidia-smi start-up
+    time.sleep(1.0)                                  # nvidia-smi start-up
     barrier()
     torch.cuda.synchronize()
-    clocks.mark("t_begin")
+    clocks.t_begin = time.time()
     l0 = ctx.launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    energy_ms = []
+    stages = []
     for _ in range(args.steps):
-        r = step_device()
-        energy_ms.append(r["ms_energy"])
+        r = step(ctx, prec, C_dev, e_dev)
+        stages.append(ctx.stage_times())
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
     launches = ctx.launch_count() - l0
-    clocks.mark("t_end")
+    clocks.t_end = time.time()
     elapsed = ev0.elapsed_time(ev1) / 1e3
     time.sleep(0.3)
     clk = clocks.stop()
+    exact = ctx.mixed_exact() if prec != capi.FP64 else True
 
     t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     elapsed = float(t.item())
-    flops = workload_flops(w)
+    flops = workload_flops(N, o, M, gradient)
     value = world * flops * args.steps / elapsed / 1e12
+    mixed_res = r
+
+    # ---- FP64 path on the same inputs (comparison and error) ---------------
+    fp64 = {}
+    if prec != capi.FP64 and not args.no_fp64:
+        step(ctx, capi.FP64, C_dev, e_dev)                       # warm
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        r64 = step(ctx, capi.FP64, C_dev, e_dev)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = t0.elapsed_time(t1)
+        if gradient:
+            e3, e64 = mixed_res.energy["total"], r64.energy["total"]
+            fp64 = {"fp64_ms_per_step": ms64, "fp64_tflops": flops / (ms64 / 1e3) / 1e12,
+                    "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps),
+                    "energy_fp64": e64, "energy_mixed": e3,
+                    "energy_error_uEh": abs(e3 - e64) * 1e6,
+                    "max_abs_dC_error": float(np.max(np.abs(mixed_res.dC_a - r64.dC_a))),
+                    "max_abs_deps_error": float(np.max(np.abs(mixed_res.deps_a - r64.deps_a))),
+                    "max_abs_dC": float(np.max(np.abs(r64.dC_a)))}
+        else:
+            fp64 = {"fp64_ms_per_step": ms64,
+                    "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps),
+                    "energy_error_uEh": abs(mixed_res["total"] - r64["total"]) * 1e6}
 
     # ---- end to end through the C ABI from pinned host buffers ------------
-    ctx_h = capi.Context(local_rank)
-    ctx_h.set_stream(stream.cuda_stream)
+    e2e = None
+    if not args.no_e2e:
+        L_host = torch.empty(L_dev.shape, dtype=torch.float64, pin_memory=True)
+        L_host.copy_(L_dev)
+        C_host = np.asfortranarray(orb.C)
+        e_host = orb.eps.copy()
+        del L_dev
+        ctx.close()
+        torch.cuda.empty_cache()
+        ctx_h = capi.Context(local_rank)
+        ctx_h.set_stream(stream.cuda_stream)
+        L_np = L_host.numpy()
 
-    def step_e2e():
-        ctx_h.set_vectors(L_host.numpy())
-        ctx_h.set_orbitals(capi.ALPHA, C_host.numpy(), e_host.numpy(), o)
-        return ctx_h.mp2_energy(kind, prec)
+        def step_e2e():
+            ctx_h.set_vectors(L_np, nbf=N)
+            ctx_h.set_orbitals(capi.ALPHA, C_host, e_host, o)
+            if gradient:
+                return ctx_h.mp2_gradient(capi.RESTRICTED, prec)       # results copied to host
+            return ctx_h.mp2_energy(capi.RESTRICTED, prec)
 
-    step_e2e()
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
         step_e2e()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    e2e_elapsed = max(wall, e0.elapsed_time(e1) / 1e3)
-    t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_elapsed = float(t.item())
-    e2e_value = world * flops * args.steps / e2e_elapsed / 1e12
-    h2d = L_host.numel() * 8 + C_host.numel() * 8 + e_host.numel() * 8
-    d2h = 8 * 7   # the energy record
-
-    # ---- roofline of the dominant kernel (pair energy) --------------------
-    peaks, peak_src = measured_peaks()
-    if w["precision"] == "fp64":
-        fp64_peak = measure_fp64_peak(torch, dev)
-        peak, peak_note = fp64_peak, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
+        barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            step_e2e()
+        torch.cuda.synchronize()
+        e2e_elapsed = time.perf_counter() - w0
+        t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+        h2d = L_np.nbytes + C_host.nbytes + e_host.nbytes
+        d2h = 8 * 7 + ((N * N + N) * 8 if gradient else 0)
+        e2e = {"value": world * flops * args.steps / e2e_elapsed / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": 1e3 * e2e_elapsed / args.steps}
+        ctx_h.close()
     else:
-        peak = peaks["bf16_tflops"] / 3.0
-        peak_note = f"bf16 dense {peak_src} / 3 (three split products)"
-    ke = flops_energy(N, o, M)
-    kms = statistics.median(energy_ms)
-    achieved = ke / (kms / 1e3) / 1e12
-    energy_check = r["total"]
+        ctx.close()
 
-    ctx_h.close()
-    ctx.close()
+    # ---- roofline of the dominant kernel ----------------------------------
+    peaks, peak_src = measured_peaks()
+    st = {k: statistics.median(s[k] for s in stages) for k in stages[0]}
+    if gradient:
+        cand = {"amplitude": ("pair_energy_tc_kernel<AMPLITUDE>", 2.0 * (N - o) ** 2 * M * o * o),
+                "gamma": ("gamma_tc_kernel", flops_gamma(N, o, M))}
+    else:
+        cand = {"pair_energy": ("pair_energy_tc_kernel<RESTRICTED>", flops_energy(N, o, M))}
+    dom = max(cand, key=lambda k: st.get(k, 0.0))
+    kname, kflops = cand[dom]
+    kms = st[dom]
+    achieved = kflops / (kms / 1e3) / 1e12 if kms > 0 else None
+    if prec == capi.FP64:
+        peak = measure_fp64_peak(torch, dev)
+        peak_note = "FP64 cuBLAS DGEMM 8192^3 measured in this run"
+    else:
+        peak = peaks["bf16_tflops_sustained"] / 3.0
+        peak_note = (f"dense 16-bit tensor peak ({peak_src}, sustained "
+                     f"{peaks['bf16_tflops_sustained']}) / 3: three products per useful product")
 
     if rank == 0:
         line = {
-            "metric": metric_name(w), "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if w["precision"] == "fp64" else "fp16x3 (scaled fixed point, exact f32 accumulate; f64 denominators, sums)",
-            "data": "synthetic",
+            "dtype": ("f64" if prec == capi.FP64 else
+                      "fp16x3 (scaled fixed point, exact f32 accumulate; f64 denominators, sums)"),
+            "data": "synthetic (seeded recipe, scaled twin, device Philox stream for L)",
             "config": {"workload": args.workload, "N": N, "o": o, "v": N - o, "M": M,
-                       "kind": w["kind"], "precision": w["precision"],
-                       "gradient": w["gradient"], "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (L %.1f GB, B %.2f GB)" % (
+                       "kind": "restricted", "precision": w["precision"], "gradient": gradient,
+                       "sigma": sigma, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (AO vectors %.1f GB, MO vectors %.2f GB)" % (
                            N * N * M * 8 / 1e9, o * (N - o) * M * 8 / 1e9),
-                       "e_corr": energy_check},
+                       "stage_ms": st, "mixed_exact_accumulation": exact, **fp64},
             "clocks": clk,
-            "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_elapsed / args.steps},
+            "e2e": e2e,
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor",
-                         "kernel": ("pair_energy_f64_kernel<RESTRICTED>" if w["precision"] == "fp64"
-                                    else "pair_energy_tc_kernel<RESTRICTED>"),
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_note,
-                         "kernel_ms": kms},
+            "roofline": {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": None, "peak_source": peak_note, "kernel_ms_per_step": kms},
         }
         if not args.no_cpu_baseline:
             try:
@@ -366,7 +415,7 @@ def bench_gpu(args, w, rank, world, local_rank):
                     line["cpu_baseline"] = {"value": fs / ts / 1e12, "unit": "TFLOP/s",
                                             "cores": nthreads, "kind": "reference",
                                             "sample": sample, "seconds": ts}
-            except Exception as ex:  # the baseline is a report, not the product
+            except Exception as ex:   # a reported baseline, not the product
                 line["cpu_baseline"] = {"value": None, "error": str(ex)}
         print(json.dumps(line))
 
@@ -374,11 +423,13 @@ def bench_gpu(args, w, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison step")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     w = WORKLOADS[args.workload]
@@ -394,7 +445,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     try:
         bench_gpu(args, w, rank, world, local_rank)
     finally:

@@ -56,6 +56,8 @@ SIGNATURES = {
     "mshqc_cd_set_stream": (_i32, [_vp, _vp]),
     "mshqc_cd_device_bytes": (_i32, [_vp, ctypes.POINTER(_i64)]),
     "mshqc_cd_launch_count": (_i32, [_vp, ctypes.POINTER(_i64)]),
+    "mshqc_cd_stage_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
+    "mshqc_cd_mixed_exact": (_i32, [_vp, ctypes.POINTER(_i32)]),
     "mshqc_cd_set_vectors": (_i32, [_vp, _vp, _i64, _i64, _i32, _i32]),
     "mshqc_cd_set_orbitals": (_i32, [_vp, _i32, _vp, _vp, _i64, _i32]),
     "mshqc_cd_transform": (_i32, [_vp, _i32, _i32, _vp, _i32]),
@@ -161,6 +163,18 @@ class Context:
         c = ctypes.c_int64(0)
         _check(self._lib.mshqc_cd_launch_count(self._h, ctypes.byref(c)))
         return int(c.value)
+
+    STAGES = ("transform", "split", "pair_energy", "amplitude", "gamma", "transposed", "other")
+
+    def stage_times(self) -> dict:
+        buf = (ctypes.c_double * 8)()
+        _check(self._lib.mshqc_cd_stage_times(self._h, buf, 8))
+        return {name: buf[k] for k, name in enumerate(self.STAGES)}
+
+    def mixed_exact(self) -> bool:
+        x = ctypes.c_int(0)
+        _check(self._lib.mshqc_cd_mixed_exact(self._h, ctypes.byref(x)))
+        return bool(x.value)
 
     # -- inputs -----------------------------------------------------------
     def set_vectors(self, L, nbf: int | None = None, layout: str = "full"):

@@ -32,6 +32,41 @@ thread_local std::string g_last_error = "";
 }
 
 namespace mshqc_cd {
+void reset_stages(mshqc_cd_ctx* ctx) {
+    for (double& t : ctx->stage_ms) t = 0.0;
+    ctx->ev_marks.clear();
+    ctx->ev_used = 0;
+}
+static cudaEvent_t next_event(mshqc_cd_ctx* ctx) {
+    if (ctx->ev_used == ctx->ev_pool.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        ctx->ev_pool.push_back(e);
+    }
+    return ctx->ev_pool[ctx->ev_used++];
+}
+void begin_stage(mshqc_cd_ctx* ctx, int stage) {
+    const size_t idx = ctx->ev_used;
+    cudaEvent_t e = next_event(ctx);
+    if (!e) return;
+    cudaEventRecord(e, ctx->stream);
+    ctx->ev_marks.push_back({stage, (int)idx});
+}
+void end_stage(mshqc_cd_ctx* ctx) {
+    cudaEvent_t e = next_event(ctx);
+    if (e) cudaEventRecord(e, ctx->stream);
+}
+void collect_stages(mshqc_cd_ctx* ctx) {
+    for (const auto& m : ctx->ev_marks) {
+        if ((size_t)m.second + 1 >= ctx->ev_used) continue;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ctx->ev_pool[m.second], ctx->ev_pool[m.second + 1]) == cudaSuccess)
+            ctx->stage_ms[m.first] += ms;
+    }
+    ctx->ev_marks.clear();
+    ctx->ev_used = 0;
+}
+
 int set_error(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
@@ -277,6 +312,20 @@ int mshqc_cd_ctx_destroy(mshqc_cd_ctx* ctx) {
 int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream) {
     CD_CHECK_CTX();
     ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+    return MSHQC_CD_OK;
+}
+
+int mshqc_cd_stage_times(mshqc_cd_ctx* ctx, double* ms_out, int n_out) {
+    CD_CHECK_CTX();
+    if (!ms_out || n_out < 0) return set_error(MSHQC_CD_ERR_ARG, "bad output");
+    for (int k = 0; k < n_out && k < 8; ++k) ms_out[k] = ctx->stage_ms[k];
+    return MSHQC_CD_OK;
+}
+
+int mshqc_cd_mixed_exact(mshqc_cd_ctx* ctx, int* exact) {
+    CD_CHECK_CTX();
+    if (!exact) return set_error(MSHQC_CD_ERR_ARG, "exact is null");
+    *exact = ctx->fixed_point_exact;
     return MSHQC_CD_OK;
 }
 

@@ -64,6 +64,11 @@ struct mshqc_cd_ctx {
     int64_t N = 0, M = 0, Mp = 0;
     bool L_set = false;
     int64_t launches = 0;           // kernels launched by this context
+    // per-stage device timing of the last call (see mshqc_cd_stage_times)
+    double stage_ms[8] = {};
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, int>> ev_marks;   // (stage, index of the start event)
+    size_t ev_used = 0;
     mshqc_cd::DevBuf L;             // [Q][N*N] FP64
     mshqc_cd::SpinState spin[2];
 
@@ -107,6 +112,9 @@ struct mshqc_cd_ctx {
         return b;
     }
     void release_all() {
+        for (auto& e : ev_pool)
+            if (e) cudaEventDestroy(e);
+        ev_pool.clear();
         L.release();
         Y.release();
         scratch.release();
@@ -136,6 +144,13 @@ struct mshqc_cd_ctx {
 };
 
 namespace mshqc_cd {
+enum Stage { ST_TRANSFORM = 0, ST_SPLIT, ST_PAIR, ST_AMPLITUDE, ST_GAMMA, ST_TRANSPOSED, ST_OTHER };
+// stage timing: begin_stage/end_stage record events on the context stream;
+// collect_stages (after a synchronize) folds them into ctx->stage_ms
+void reset_stages(mshqc_cd_ctx* ctx);
+void begin_stage(mshqc_cd_ctx* ctx, int stage);
+void end_stage(mshqc_cd_ctx* ctx);
+void collect_stages(mshqc_cd_ctx* ctx);
 int set_error(int code, const std::string& msg);
 int cuda_error(cudaError_t e, const char* what);
 int upload(mshqc_cd_ctx* ctx, void* dst, const void* src, size_t nbytes);

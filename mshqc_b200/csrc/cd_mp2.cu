@@ -193,6 +193,7 @@ int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
     a.partial = ctx->partial.as<double>();
     a.partial2 = ctx->partial.as<double>() + units;
     const size_t smem = pair_f64_detail::SMEM_BYTES;
+    begin_stage(ctx, ST_PAIR);
     if (mode == PAIR_RESTRICTED) {
         CD_CUDA(cudaFuncSetAttribute(pair_energy_f64_kernel<PAIR_RESTRICTED>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -206,6 +207,7 @@ int pair_pass_f64(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         pair_energy_f64_kernel<PAIR_OPPOSITE_SPIN><<<(unsigned)units, 256, smem, ctx->stream>>>(a);
     }
+    end_stage(ctx);
     CD_CUDA(cudaGetLastError());
     ctx->launches++;
     CD_RC(reduce_and_collect(ctx, mode, t, units, npairs, nblocks, ox, oy, total, pair_mat, total_os));
@@ -362,7 +364,11 @@ int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
         const double bx = std::sqrt(X.max_norm_hi * Y.max_norm_lo) + std::sqrt(X.max_norm_lo * Y.max_norm_hi);
         if (!(bhh < lim && bx < lim)) ctx->fixed_point_exact = 0;
     }
-    if (mode == PAIR_OPPOSITE_SPIN) CD_RC(opposite_spin_diag(ctx));
+    if (mode == PAIR_OPPOSITE_SPIN) {
+        begin_stage(ctx, ST_SPLIT);
+        CD_RC(opposite_spin_diag(ctx));
+        end_stage(ctx);
+    }
     PairTcArgs a{};
     a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
     a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
@@ -388,12 +394,14 @@ int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
     a.err = ctx->flag.as<int>();
     const int grid = (int)std::min<int64_t>(units, ctx->num_sms);
     cudaError_t e;
+    begin_stage(ctx, ST_PAIR);
     if (mode == PAIR_RESTRICTED)
         e = launch_tc<PAIR_RESTRICTED>(a, grid, ctx->stream);
     else if (mode == PAIR_SAME_SPIN)
         e = launch_tc<PAIR_SAME_SPIN>(a, grid, ctx->stream);
     else
         e = launch_tc<PAIR_OPPOSITE_SPIN>(a, grid, ctx->stream);
+    end_stage(ctx);
     if (e != cudaSuccess) return cuda_error(e, "pair_energy_tc_kernel launch");
     ctx->launches++;
     int herr = 0;
@@ -413,16 +421,23 @@ int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
     if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_FP16X3)
         return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
     if (!s.B64_valid) {
+        begin_stage(ctx, ST_TRANSFORM);
         CD_RC(transform_f64(ctx, spin));
+        end_stage(ctx);
         s.B16_valid = false;
     }
-    if (precision == MSHQC_CD_FP16X3 && !s.B16_valid) CD_RC(split_fixed(ctx, spin));
+    if (precision == MSHQC_CD_FP16X3 && !s.B16_valid) {
+        begin_stage(ctx, ST_SPLIT);
+        CD_RC(split_fixed(ctx, spin));
+        end_stage(ctx);
+    }
     return MSHQC_CD_OK;
 }
 
 int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out) {
     std::memset(out, 0, sizeof(*out));
     ctx->fixed_point_exact = 1;
+    reset_stages(ctx);
     auto pass = [&](int mode, int sx, int sy, double* tot, std::vector<double>& pm,
                     double* tot_os) {
         return precision == MSHQC_CD_FP16X3 ? pair_pass_tc(ctx, mode, sx, sy, tot, pm, tot_os)
@@ -454,6 +469,7 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
     }
     CD_CUDA(cudaEventRecord(e2, ctx->stream));
     CD_CUDA(cudaEventSynchronize(e2));
+    collect_stages(ctx);
     float t01 = 0, t12 = 0;
     CD_CUDA(cudaEventElapsedTime(&t01, e0, e1));
     CD_CUDA(cudaEventElapsedTime(&t12, e1, e2));
@@ -551,7 +567,9 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
         a.partial = ctx->partial.as<double>() + (int64_t)i0 * units_per_i;
         a.nb = nb;
         const int64_t units = (int64_t)nbi * units_per_i;
+        begin_stage(ctx, ST_AMPLITUDE);
         amp_f64_kernel<<<(unsigned)units, 256, smem, ctx->stream>>>(a);
+        end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
         // Gamma[(i,a)][Q] = sum_{(j,b)} tt[(i,a)][(j,b)] B[(j,b)][Q]
@@ -561,7 +579,9 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
         g.B = s.B64.as<double>();  g.ldb = Mp;  g.sB = 0;
         g.C = ctx->gam[0].as<double>() + (int64_t)i0 * vp * Mp;  g.ldc = Mp;  g.sC = 0;
         g.alpha = 1.0;  g.beta = 0.0;
+        begin_stage(ctx, ST_GAMMA);
         CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        end_stage(ctx);
         ctx->launches++;
     }
     reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * units_per_i),
@@ -570,7 +590,9 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
     ctx->launches++;
     CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 
+    begin_stage(ctx, ST_TRANSPOSED);
     CD_RC(transposed_transforms(ctx, dC));
+    end_stage(ctx);
     CD_CUDA(cudaStreamSynchronize(ctx->stream));
     return MSHQC_CD_OK;
 }
@@ -592,8 +614,10 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
     {
         const int64_t threads = (KA / 16) * RQ * 2;
         const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
+        begin_stage(ctx, ST_SPLIT);
         bt_split_kernel<<<blocks, 256, 0, ctx->stream>>>(s.B64.as<double>(), vp, Mp, (int)v, (int)M, o,
                                                          VR, RQ, bth, btl);
+        end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
@@ -645,7 +669,9 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
         a.i0 = i0;
         a.deps = deps;
         const int grid = (int)std::min<int64_t>(units, ctx->num_sms);
+        begin_stage(ctx, ST_AMPLITUDE);
         cudaError_t e = launch_tc<PAIR_AMPLITUDE>(a, grid, ctx->stream);
+        end_stage(ctx);
         if (e != cudaSuccess) return cuda_error(e, "amplitude kernel launch");
         ctx->launches++;
         GammaTcArgs g{};
@@ -662,7 +688,9 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
         const size_t gsm = gamma_tc::SMEM_BYTES;
         CD_CUDA(cudaFuncSetAttribute(gamma_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
         const int ggrid = (int)std::min<int64_t>((int64_t)g.nrb * g.nqb, ctx->num_sms);
+        begin_stage(ctx, ST_GAMMA);
         gamma_tc_kernel<<<ggrid, gamma_tc::THREADS, gsm, ctx->stream>>>(g);
+        end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
@@ -678,7 +706,9 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
         return set_error(MSHQC_CD_ERR_TIMEOUT, "tensor-core backward gave up waiting (site " +
                                                    std::to_string(herr[0] ? herr[0] : herr[2]) + ")");
     if (herr[1]) ctx->fixed_point_exact = 0;
+    begin_stage(ctx, ST_TRANSPOSED);
     CD_RC(transposed_transforms(ctx, dC));
+    end_stage(ctx);
     return MSHQC_CD_OK;
 }
 
@@ -693,6 +723,7 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
     CD_RC(require_inputs(ctx, 0));
     const int64_t N = ctx->N;
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    reset_stages(ctx);
     CD_CUDA(cudaEventRecord(e0, ctx->stream));
     CD_RC(ensure_transform(ctx, 0, precision));
     CD_CUDA(cudaEventRecord(e1, ctx->stream));
@@ -707,6 +738,7 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
         CD_RC(gradient_restricted_tc(ctx, dC, de, &energy));
     CD_CUDA(cudaEventRecord(e2, ctx->stream));
     CD_CUDA(cudaEventSynchronize(e2));
+    collect_stages(ctx);
     if (e_out) {
         std::memset(e_out, 0, sizeof(*e_out));
         e_out->total = energy;

@@ -149,3 +149,28 @@ def default_core_hamiltonian(inp: CDInputs) -> np.ndarray:
         K += Lq @ Pa @ Lq
     F = (a.C * a.eps[None, :]) @ a.C.T
     return F - J + K
+
+
+def make_vectors_device(N: int, M: int, seed: int, sigma: float, device, chunk: int = 64):
+    """The same recipe as make_vectors, drawn on the device with a seeded
+    torch (Philox) generator: L^Q = sigma s_Q (X + X^T)/2.  Returns an (M, N*N)
+    float64 CUDA tensor.  Used for workloads too large to draw on the host;
+    the stream differs from numpy's, the distribution is the same."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    s = torch.from_numpy(scale_factors(M) * sigma).to(device)
+    L = torch.empty((M, N * N), dtype=torch.float64, device=device)
+    for q0 in range(0, M, chunk):
+        q1 = min(M, q0 + chunk)
+        X = torch.randn((q1 - q0, N, N), dtype=torch.float64, device=device, generator=g)
+        X = 0.5 * (X + X.transpose(1, 2))
+        X *= s[q0:q1, None, None]
+        L[q0:q1] = X.reshape(q1 - q0, N * N)
+        del X
+    return L
+
+
+def make_orbitals(N: int, nocc: int, seed: int) -> SpinOrbitals:
+    rng = np.random.default_rng(seed)
+    return SpinOrbitals(_orthogonal(rng, N), _orbital_energies(rng, N, nocc), nocc)
