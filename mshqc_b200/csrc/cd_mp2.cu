@@ -41,6 +41,16 @@ namespace mshqc_cd {
 
 namespace {
 
+// out[k] = alpha * sum_s parts[s * n + k], in a fixed order
+__global__ void sum_partials_kernel(const double* __restrict__ parts, int S, int64_t n, double alpha,
+                                    double* __restrict__ out) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double acc = 0.0;
+    for (int s = 0; s < S; ++s) acc += parts[(int64_t)s * n + k];
+    out[k] = alpha * acc;
+}
+
 int require_inputs(mshqc_cd_ctx* ctx, int spin) {
     if (!ctx->L_set) return set_error(MSHQC_CD_ERR_STATE, "Cholesky vectors not set");
     if (!ctx->spin[spin].set)
@@ -520,15 +530,35 @@ int transposed_transforms(mshqc_cd_ctx* ctx, double* dC) {
         ctx->launches++;
         ctx->Y_spin = -1;
     }
-    // dC[mu, i] = 4 sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]
+    // dC[mu, i] = 4 sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]: only o rows, so the
+    // long K = M*N is split over S independent partial products (batched
+    // GEMM) that a deterministic reduction adds up
     {
+        const int64_t K = M * N;
+        const int64_t tiles = cdiv(o, 64) * cdiv(N, 64);
+        const int64_t S = std::max<int64_t>(1, std::min<int64_t>(256, cdiv(4 * ctx->num_sms, tiles)));
+        const int64_t Kc = (K / S) / 16 * 16, Krem = K - S * Kc;   // even chunks keep 16-byte copies
+        CD_ALLOC(ctx->W, sizeof(double) * (size_t)(S * o * N), false);
         GemmF64Args g{};
-        g.M = (int)o;  g.N = (int)N;  g.K = (int)(M * N);  g.batch = 1;
-        g.A = ctx->Y.as<double>();  g.lda = M * N;  g.sA = 0;
-        g.B = ctx->L.as<double>();  g.ldb = N;  g.sB = 0;
-        g.C = dC;  g.ldc = N;  g.sC = 0;
-        g.alpha = 4.0;  g.beta = 0.0;
+        g.M = (int)o;  g.N = (int)N;  g.K = (int)Kc;  g.batch = (int)S;
+        g.A = ctx->Y.as<double>();  g.lda = M * N;  g.sA = Kc;
+        g.B = ctx->L.as<double>();  g.ldb = N;  g.sB = Kc * N;
+        g.C = ctx->W.as<double>();  g.ldc = N;  g.sC = o * N;
+        g.alpha = 1.0;  g.beta = 0.0;
         CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+        if (Krem > 0) {
+            GemmF64Args t = g;
+            t.K = (int)Krem;  t.batch = 1;
+            t.A = ctx->Y.as<double>() + S * Kc;
+            t.B = ctx->L.as<double>() + S * Kc * N;
+            t.beta = 1.0;
+            CD_CUDA(gemm_f64(t, true, false, ctx->stream));
+            ctx->launches++;
+        }
+        sum_partials_kernel<<<(unsigned)cdiv(o * N, 256), 256, 0, ctx->stream>>>(
+            ctx->W.as<double>(), (int)S, o * N, 4.0, dC);
+        CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
     return MSHQC_CD_OK;
