@@ -16,6 +16,7 @@
 #include "split_bf16.cuh"
 #include "backward_f64.cuh"
 #include "gamma_tc.cuh"
+#include "vtile_tc.cuh"
 
 namespace mshqc_cd {
 
@@ -651,58 +652,55 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
-    // occupied block size for the staging (2 x BF16 per element)
+    // occupied block size: FP32 integral staging S plus the BF16 hi/lo tt
+    const int64_t nby = cdiv(VR, 256), VS = nby * 256, nt = VR / 32;
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_i = sizeof(uint16_t) * (size_t)VR * KA;
-    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 6, size_t(24) << 30));
+    const size_t per_i_amp = sizeof(uint16_t) * (size_t)VR * KA;
+    const size_t per_i_s = sizeof(float) * (size_t)VR * (size_t)(o * VS);
+    const size_t per_i = 2 * per_i_amp + per_i_s;
+    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 3, size_t(40) << 30));
     const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(budget / per_i)));
-    CD_ALLOC(ctx->amp, per_i * bi, false);
-    CD_ALLOC(ctx->amp2, per_i * bi, false);
+    CD_ALLOC(ctx->amp, per_i_amp * bi, false);
+    CD_ALLOC(ctx->amp2, per_i_amp * bi, false);
+    CD_ALLOC(ctx->W, per_i_s * bi, false);
     CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, true);
     CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
     CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
-    const int64_t units_per_i = o * nblk * nblk;
-    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), false);
+    const int64_t tiles_per_i = o * nt * nt;
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * tiles_per_i), false);
+    const size_t vsm = vtile_tc::SMEM_BYTES;
+    CD_CUDA(cudaFuncSetAttribute(vtile_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
     for (int i0 = 0; i0 < o; i0 += bi) {
         const int nbi = (int)std::min<int64_t>(bi, o - i0);
-        UnitTables t = make_tables_amp(i0, nbi, (int)o, (int)nblk);
-        const int npairs = (int)t.pairs.size(), nblocks = (int)t.blocks.size();
-        CD_ALLOC(ctx->tables, sizeof(int2) * (t.pairs.size() + t.blocks.size()), false);
-        int2* dpairs = ctx->tables.as<int2>();
-        CD_CUDA(cudaMemcpyAsync(dpairs, t.pairs.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice,
-                                ctx->stream));
-        CD_CUDA(cudaMemcpyAsync(dpairs + npairs, t.blocks.data(), sizeof(int2) * nblocks,
-                                cudaMemcpyHostToDevice, ctx->stream));
-        const int64_t units = (int64_t)npairs * nblocks;
-        PairTcArgs a{};
+        // (ia|jb) for the rows i of this block and every j, each tile once
+        VtileArgs a{};
         a.Xhi = s.Bhi.as<uint16_t>();  a.Xlo = s.Blo.as<uint16_t>();
-        a.Yhi = a.Xhi;  a.Ylo = a.Xlo;
-        a.ex = s.expo.as<int>();  a.ey = a.ex;
-        a.diag = s.diag.as<double>();
-        a.rows_x = a.rows_y = (int)s.vp16;
-        a.nqc = (int)(Mp / 16);
-        a.vx = a.vy = (int)v;
-        a.diag_o = (int)o;  a.diag_v = (int)v;
-        a.eox = s.eps.as<double>();  a.evx = a.eox + o;
-        a.eoy = a.eox;  a.evy = a.evx;
-        a.pairs = dpairs;  a.blocks = dpairs + npairs;  a.nblocks = nblocks;
-        a.units = units;
-        a.partial = ctx->partial.as<double>() + (int64_t)i0 * units_per_i;
-        a.partial2 = nullptr;
+        a.ex = s.expo.as<int>();  a.diag = s.diag.as<double>();
+        a.rows = (int)s.vp16;  a.nqc = (int)(Mp / 16);
+        a.o = (int)o;  a.v = (int)v;  a.VR = (int)VR;  a.i0 = i0;  a.nbi = nbi;
+        a.nbx = (int)nblk;  a.nby = (int)nby;  a.VS = (int)VS;
+        a.S = ctx->W.as<float>();
         a.err = ctx->flag.as<int>();
-        a.amp_hi = ctx->amp.as<uint16_t>();
-        a.amp_lo = ctx->amp2.as<uint16_t>();
-        a.amp_rows = (long long)bi * VR;
-        a.VR = (int)VR;
-        a.i0 = i0;
-        a.deps = deps;
-        const int grid = (int)std::min<int64_t>(units, ctx->num_sms);
+        const int64_t vunits = (int64_t)nbi * o * nblk * nby;
+        const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
         begin_stage(ctx, ST_AMPLITUDE);
-        cudaError_t e = launch_tc<PAIR_AMPLITUDE>(a, grid, ctx->stream);
+        vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+        // tt = (2V - V^T)/D as BF16 hi/lo, dE/de, energy partials
+        AmpElemArgs e{};
+        e.S = ctx->W.as<float>();
+        e.o = (int)o;  e.v = (int)v;  e.VR = (int)VR;  e.VS = (int)VS;  e.i0 = i0;  e.nbi = nbi;
+        e.eo = s.eps.as<double>();  e.ev = e.eo + o;
+        e.Ahi = ctx->amp.as<uint16_t>();  e.Alo = ctx->amp2.as<uint16_t>();
+        e.RA = (long long)bi * VR;
+        e.deps = deps;
+        e.partial = ctx->partial.as<double>() + (int64_t)i0 * tiles_per_i;
+        amp_elem_kernel<<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
         end_stage(ctx);
-        if (e != cudaSuccess) return cuda_error(e, "amplitude kernel launch");
+        CD_CUDA(cudaGetLastError());
         ctx->launches++;
         GammaTcArgs g{};
         g.Ahi = ctx->amp.as<uint16_t>();  g.Alo = ctx->amp2.as<uint16_t>();
@@ -724,7 +722,7 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
-    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * units_per_i),
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * tiles_per_i),
                                                    ctx->totals.as<double>());
     CD_CUDA(cudaGetLastError());
     ctx->launches++;

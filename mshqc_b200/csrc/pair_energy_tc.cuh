@@ -265,7 +265,6 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
         const int etid = threadIdx.x - 64;            // 0..127
         uint32_t acc_phase = 0;
         for (long long u = first; u < p.units; u += step) {
-            if (*abort_flag) break;
             const int2 ij = p.pairs[u / p.nblocks];
             const int2 xy = p.blocks[u % p.nblocks];
             const int i = ij.x, j = ij.y;
@@ -292,9 +291,12 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                 eb_s[c] = eb;
                 cs_s[c] = cs;
             }
-            asm volatile("bar.sync 1, 128;\n" ::: "memory");
-            if (!mbar_wait_bounded(tmem_full, acc_phase, kWaitLimitNs)) {
-                atomicExch(p.err, 4);
+            // the four epilogue warps leave together (a named barrier must
+            // never wait for a warp that already left the loop)
+            if (bar_any(1, 128, *abort_flag != 0)) break;
+            const bool got = mbar_wait_bounded(tmem_full, acc_phase, kWaitLimitNs);
+            if (bar_any(1, 128, !got)) {
+                if (!got) atomicExch(p.err, 4);
                 *abort_flag = 1;
                 break;
             }

@@ -54,6 +54,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
+// Named barrier `id` over `nthreads` threads that also returns whether ANY of
+// them passed pred = true, so a group of warps leaves a loop together.
+__device__ __forceinline__ bool bar_any(int id, int nthreads, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, %2, %3, q;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
 // ---- 1-D bulk copy (no multicast) -----------------------------------------
 // dst / src 16-byte aligned, bytes a multiple of 16; completion counted on bar.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
