@@ -149,6 +149,45 @@ MSHQC_CD_API int mshqc_cd_mp2_gradient(mshqc_cd_ctx* ctx, int kind, int precisio
                           mshqc_cd_energy* e_out, double* dC_a, double* dC_b,
                           double* deps_a, double* deps_b, int where);
 
+/* --- allocation-free energy (no counterpart in the reference) --------- */
+/* Size of the static device scratch of mshqc_cd_rmp2_energy_noalloc. */
+#define MSHQC_CD_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* The FP64 closed-shell MP2 energy of mshqc_cd_mp2_energy(RESTRICTED, FP64)
+ * from MO vectors already on the device, allocating nothing: no context, no
+ * cudaMalloc / cudaFree, no allocating library call.  It is meant for callers
+ * that cannot allocate at that point: code inside a framework or memory pool
+ * that owns the whole device budget, and code on a latency-critical stream
+ * (cudaMalloc and cudaFree synchronize the device and stall other streams).
+ *
+ * Scratch: one static device array of MSHQC_CD_NOALLOC_SCRATCH_BYTES
+ * (16 MiB) per device.  A call needs
+ *     roundup(8 (P + K), 256) + 16 P K + 16 P  bytes,
+ *     P = nocc (nocc + 1) / 2,  K = nb (nb + 1) / 2,  nb = ceil(nvir / 64)
+ * (nocc = 100, nvir = 900 needs 9.8 MB); larger sizes are rejected with
+ * MSHQC_CD_ERR_ARG and a message, before the device is touched.
+ *
+ * B       device, nocc * vp * Mp doubles, element (i * vp + a) * Mp + Q with
+ *         vp = ceil(nvir / 64) * 64, Mp = ceil(nvec / 16) * 16; the padding
+ *         (a >= nvir or Q >= nvec) must be zero.
+ * eps     device, nocc + nvir orbital energies, occupied first.
+ * energy  device, 2 doubles, written in stream order: [0] E_corr,
+ *         [1] its opposite-spin part.
+ * stream  a cudaStream_t, or NULL for the legacy default stream.  The call
+ *         returns once its kernels are queued; synchronize the stream before
+ *         reading energy.
+ *
+ * Set-up happens on the first call with each device current (it looks up the
+ * scratch address and the kernel attributes): make that first call outside
+ * any stream capture.  No scratch word needs to start at zero: a call writes
+ * all the scratch it reads before reading it.  All calls on one device share
+ * the scratch, so calls that overlap in time (different streams or host
+ * threads) race on it: order them (one stream, or events).  Inputs are not
+ * checked for NaN/Inf. */
+MSHQC_CD_API int mshqc_cd_rmp2_energy_noalloc(const double* B, const double* eps, int64_t nocc,
+                                              int64_t nvir, int64_t nvec, double* energy,
+                                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,7 @@ SIGNATURES = {
     "mshqc_cd_pair_energies": (_i32, [_vp, _i32, _vp, _i32]),
     "mshqc_cd_mp2_gradient": (_i32, [_vp, _i32, _i32, ctypes.POINTER(Energy), _vp, _vp, _vp,
                                      _vp, _i32]),
+    "mshqc_cd_rmp2_energy_noalloc": (_i32, [_vp, _vp, _i64, _i64, _i64, _vp, _vp]),
 }
 
 _lib = None
@@ -246,6 +247,33 @@ class Context:
             _ptr(dCb) if dCb is not None else None, _ptr(dea),
             _ptr(deb) if deb is not None else None, HOST))
         return Gradient(e.as_dict(), dCa, dCb, dea, deb)
+
+
+def noalloc_shape(nocc: int, nvir: int, nvec: int) -> tuple[int, int, int]:
+    """Shape (nocc, vp, Mp) of the zero-padded MO vectors that
+    mshqc_cd_rmp2_energy_noalloc reads."""
+    return nocc, -(-nvir // 64) * 64, -(-nvec // 16) * 16
+
+
+def rmp2_energy_noalloc(B, eps, nocc: int, nvir: int, nvec: int, energy, stream=None) -> None:
+    """Queue the allocation-free FP64 closed-shell energy on CUDA tensors.
+
+    B: float64 CUDA tensor of noalloc_shape(nocc, nvir, nvec), zero padded;
+    eps: float64 CUDA tensor (nocc + nvir,); energy: float64 CUDA tensor (2,)
+    receiving [E_corr, opposite-spin part] in stream order.  stream: a
+    torch.cuda.Stream (default: the current stream).  Nothing is allocated
+    by the call; synchronize the stream before reading energy."""
+    import torch
+    for name, t in (("B", B), ("eps", eps), ("energy", energy)):
+        if not (_is_torch_cuda(t) and t.dtype == torch.float64 and t.is_contiguous()):
+            raise ValueError(f"{name} must be a contiguous float64 CUDA tensor")
+    if tuple(B.shape) != noalloc_shape(nocc, nvir, nvec):
+        raise ValueError(f"B has shape {tuple(B.shape)}, expected {noalloc_shape(nocc, nvir, nvec)}")
+    if stream is None:
+        stream = torch.cuda.current_stream(B.device)
+    with torch.cuda.device(B.device):
+        _check(load_library().mshqc_cd_rmp2_energy_noalloc(
+            B.data_ptr(), eps.data_ptr(), nocc, nvir, nvec, energy.data_ptr(), stream.cuda_stream))
 
 
 def exported_symbols_from_header(path: str = HEADER) -> list[str]:
