@@ -1,0 +1,192 @@
+// Element-wise amplitude pass of the MP2 backward.
+//
+// Input: a staging block of integrals S[(i - i0, a)][(j, b)] = (ia|jb) for
+// the occupied rows i of one block and every j (FP32 from vtile_tc.cuh, or
+// FP64 from the FP64 GEMM).  One CTA of 256 threads takes one 32 x 32 tile of
+// (a, b) of one pair (i, j); with D = e_i + e_j - e_a - e_b (|D| < 1e-12
+// skipped, reference src/mp2/cholesky_rmp2.cc:139):
+//
+//   RESTRICTED     V = (ia|jb), W = (ib|ja); t = V/D, amplitude tt = (2V - W)/D,
+//                  energy V tt, r = t tt          (dE/dB = 4 Gamma)
+//   SAME_SPIN      g = V - W, amplitude t = g/D, energy g t / 4, r = t^2 / 4
+//                                                  (dE/dB = 2 Gamma)
+//   OPPOSITE_SPIN  X alpha, Y beta; amplitude t = V/D, energy V t, r = t^2
+//                  (dE/dB_alpha = 2 Gamma_alpha, dE/dB_beta = 2 Gamma_beta)
+//
+// The energies are those of reference src/mp2/cholesky_rmp2.cc:135-151 and
+// src/mp2/cholesky_ump2.cc:316-346, :436-453 summed over ordered pairs.
+// Gamma = amplitude x B is formed afterwards by a GEMM with K = (j, b); this
+// pass writes the amplitude operand of that GEMM: BF16 hi/lo in the blocked
+// K-major layout of the tensor-core Gamma kernel (SPLIT), or FP64 row-major
+// [(i - i0, a)][(j, b)] for the FP64 GEMM.  OPPOSITE_SPIN with SPLIT also
+// writes the transposed operand [(j, b)][(i - i0, a)] for Gamma_beta.
+// dE/de gets -r on i and j and +r on a and b (atomics); the tile's energy goes
+// to partial[tile] and a deterministic reduction adds the tiles up.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <type_traits>
+
+#include "cd_common.cuh"
+
+namespace mshqc_cd {
+
+enum AmpMode { AMP_RESTRICTED = 0, AMP_SAME_SPIN = 1, AMP_OPPOSITE_SPIN = 2 };
+
+struct AmpElemArgs {
+    const void* S;          // float (SPLIT) or double
+    long long ldS;          // row length of S
+    int rsx;                // rows per occupied i in S and in the output (multiple of 32)
+    int csy;                // columns per occupied j in S
+    int ksy;                // output K per occupied j (multiple of 32, <= csy)
+    int ox, oy, vx, vy, i0, nbi;
+    const double* eox; const double* evx;   // energies of the row spin
+    const double* eoy; const double* evy;   // of the column spin
+    uint16_t* Ahi; uint16_t* Alo; long long RA;   // SPLIT: rows R = ii*rsx + a, K = j*ksy + b
+    uint16_t* Thi; uint16_t* Tlo; long long RT;   // SPLIT, OPPOSITE_SPIN: rows j*ksy + b, K = ii*rsx + a
+    double* A64; long long ldA;                   // FP64: [R][K]
+    double* deps_x; double* deps_y;               // occupied then virtual (same array when X = Y)
+    double* partial;        // [nbi * oy * (rsx/32) * (ksy/32)]
+};
+
+namespace amp_detail {
+// blocked K-major element offset of (row R, column k): 16-wide K chunks of
+// RA rows, 8 x 8 core matrices (the operand layout of the Gamma kernel)
+__device__ __forceinline__ long long blocked_offset(long long R, long long k, long long RA) {
+    return (k >> 4) * RA * 16 + ((R >> 3) * 16 + ((k & 15) >> 3) * 8 + (R & 7)) * 8 + (k & 7);
+}
+
+// eight consecutive-k values -> one 16-byte hi row and one 16-byte lo row
+__device__ __forceinline__ void store_hilo8(const double* t, uint16_t* hi, uint16_t* lo) {
+    uint32_t wh[4], wl[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const __nv_bfloat16 h0 = __double2bfloat16(t[2 * e]), h1 = __double2bfloat16(t[2 * e + 1]);
+        const __nv_bfloat16 l0 = __double2bfloat16(t[2 * e] - (double)__bfloat162float(h0));
+        const __nv_bfloat16 l1 = __double2bfloat16(t[2 * e + 1] - (double)__bfloat162float(h1));
+        wh[e] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        wl[e] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    *reinterpret_cast<uint4*>(hi) = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+    *reinterpret_cast<uint4*>(lo) = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+}
+}  // namespace amp_detail
+
+template <int MODE, bool SPLIT>
+__global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
+    using TS = typename std::conditional<SPLIT, float, double>::type;
+    __shared__ TS Vt[32][33];
+    __shared__ TS Wt[MODE == AMP_OPPOSITE_SPIN ? 1 : 32][33];
+    __shared__ double T[32][33];
+    __shared__ double rsum_s[32], csum_s[32], red_e[8], red_r[8];
+    const TS* S = static_cast<const TS*>(p.S);
+    const int ta = p.rsx / 32, tb = p.ksy / 32;
+    const long long tile = blockIdx.x;
+    const long long pr = tile / ((long long)ta * tb);
+    const int tab = (int)(tile % ((long long)ta * tb));
+    const int ii = (int)(pr / p.oy), j = (int)(pr % p.oy), i = p.i0 + ii;
+    const int a0 = (tab / tb) * 32, b0 = (tab % tb) * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+    if (threadIdx.x < 32) {
+        rsum_s[threadIdx.x] = 0.0;
+        csum_s[threadIdx.x] = 0.0;
+    }
+#pragma unroll
+    for (int r = ty; r < 32; r += 8) {
+        Vt[r][tx] = S[((long long)ii * p.rsx + a0 + r) * p.ldS + (long long)j * p.csy + b0 + tx];
+        if (MODE != AMP_OPPOSITE_SPIN)   // (ib|ja): rows (i, b), columns (j, a)
+            Wt[r][tx] = S[((long long)ii * p.rsx + b0 + r) * p.ldS + (long long)j * p.csy + a0 + tx];
+    }
+    __syncthreads();
+    const double eij = p.eox[i] + p.eoy[j];
+    double esum = 0.0, rtot = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = ty * 4 + k;
+        const int a = a0 + r, b = b0 + tx;
+        double amp = 0.0, rr = 0.0;
+        if (a < p.vx && b < p.vy) {
+            const double D = eij - p.evx[a] - p.evy[b];
+            if (fabs(D) >= kDenomSkip) {
+                const double V = (double)Vt[r][tx];
+                const double rD = 1.0 / D;
+                if (MODE == AMP_RESTRICTED) {
+                    const double W = (double)Wt[tx][r];
+                    const double t = V * rD;
+                    amp = (2.0 * V - W) * rD;
+                    rr = t * amp;
+                    esum = fma(V, amp, esum);
+                } else if (MODE == AMP_SAME_SPIN) {
+                    const double W = (double)Wt[tx][r];
+                    const double g = V - W;
+                    amp = g * rD;
+                    rr = 0.25 * amp * amp;
+                    esum = fma(0.25 * g, amp, esum);
+                } else {
+                    amp = V * rD;
+                    rr = amp * amp;
+                    esum = fma(V, amp, esum);
+                }
+            }
+        }
+        T[r][tx] = amp;
+        rtot += rr;
+        double rs = rr;
+#pragma unroll
+        for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
+        if (tx == 0) rsum_s[r] = rs;
+        if (rr != 0.0) atomicAdd(&csum_s[tx], rr);
+        if (!SPLIT) p.A64[((long long)ii * p.rsx + a) * p.ldA + (long long)j * p.ksy + b] = amp;
+    }
+    __syncthreads();
+    if (SPLIT) {
+        // 32 rows x 4 groups of 8 K = 128 core-matrix rows per operand
+        if (threadIdx.x < 128) {
+            const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
+            const long long R = (long long)ii * p.rsx + a0 + r;
+            const long long kc = (long long)j * p.ksy + b0 + g * 8;
+            const long long off = amp_detail::blocked_offset(R, kc, p.RA);
+            amp_detail::store_hilo8(&T[r][g * 8], p.Ahi + off, p.Alo + off);
+        } else if (MODE == AMP_OPPOSITE_SPIN) {
+            const int w = threadIdx.x - 128;
+            const int r = w >> 2, g = w & 3;   // r: b offset, g: group of 8 a
+            const long long R = (long long)j * p.ksy + b0 + r;
+            const long long kc = (long long)ii * p.rsx + a0 + g * 8;
+            const long long off = amp_detail::blocked_offset(R, kc, p.RT);
+            double col[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) col[e] = T[g * 8 + e][r];
+            amp_detail::store_hilo8(col, p.Thi + off, p.Tlo + off);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        esum += __shfl_xor_sync(0xffffffffu, esum, off);
+        rtot += __shfl_xor_sync(0xffffffffu, rtot, off);
+    }
+    if (tx == 0) {
+        red_e[ty] = esum;
+        red_r[ty] = rtot;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int a = a0 + threadIdx.x, b = b0 + threadIdx.x;
+        if (a < p.vx && rsum_s[threadIdx.x] != 0.0) atomicAdd(&p.deps_x[p.ox + a], rsum_s[threadIdx.x]);
+        if (b < p.vy && csum_s[threadIdx.x] != 0.0) atomicAdd(&p.deps_y[p.oy + b], csum_s[threadIdx.x]);
+    }
+    if (threadIdx.x == 0) {
+        double e = 0.0, r = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            e += red_e[w];
+            r += red_r[w];
+        }
+        p.partial[tile] = e;
+        if (r != 0.0) {
+            atomicAdd(&p.deps_x[i], -r);
+            atomicAdd(&p.deps_y[j], -r);
+        }
+    }
+}
+
+}  // namespace mshqc_cd

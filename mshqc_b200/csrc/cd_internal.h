@@ -83,9 +83,11 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf flag;          // error / NaN flags
     mshqc_cd::DevBuf amp;           // backward: staged amplitudes
     mshqc_cd::DevBuf gam[2];        // backward: Gamma per spin
-    mshqc_cd::DevBuf BT;            // backward: transposed MO vectors (hi/lo BF16)
+    mshqc_cd::DevBuf BT;            // backward: transposed MO vectors (hi/lo BF16), alpha
+    mshqc_cd::DevBuf BT_b;          // backward: the same for beta
     mshqc_cd::DevBuf amp2;          // backward: second half of the staging (lo)
-    mshqc_cd::DevBuf W;             // backward: C_vir-contracted Gamma
+    mshqc_cd::DevBuf ampT, ampT2;   // backward: transposed opposite-spin amplitudes (hi, lo)
+    mshqc_cd::DevBuf W;             // backward: integral staging / C_vir-contracted Gamma
     mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
     mshqc_cd::DevBuf diag_os;       // sum_Q B_alpha[i][a] B_beta[i][a] (opposite-spin diagonal)
     bool diag_os_valid = false;
@@ -126,6 +128,9 @@ struct mshqc_cd_ctx {
         amp.release();
         BT.release();
         amp2.release();
+        BT_b.release();
+        ampT.release();
+        ampT2.release();
         W.release();
         for (auto& s : spin) {
             s.C.release();

@@ -17,6 +17,7 @@
 #include "backward_f64.cuh"
 #include "gamma_tc.cuh"
 #include "vtile_tc.cuh"
+#include "amp_elem.cuh"
 
 namespace mshqc_cd {
 
@@ -495,27 +496,28 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
 // ---------------------------------------------------------------------------
 namespace {
 
-// dE/dC from Gamma (in ctx->gam[0], [o][vp][Mp] FP64): dE/dB = 4 Gamma,
+// dE/dC of one spin from Gamma (ctx->gam[spin], [o][vp][Mp] FP64) with
+// dE/dB = scale * Gamma (4 restricted, 2 unrestricted):
 // dC[nu, o+a] = sum_{i,Q} dE/dB[i][a][Q] Y[i][Q][nu],
 // dC[mu, i]   = sum_{Q,nu} L[Q][nu][mu] sum_a dE/dB[i][a][Q] C[nu, o+a].
-int transposed_transforms(mshqc_cd_ctx* ctx, double* dC) {
-    SpinState& s = ctx->spin[0];
+int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC) {
+    SpinState& s = ctx->spin[spin];
     const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
-    // dE/dB = 4 Gamma.  Y[i][Q][nu] (half-transformed vectors) is needed.
-    if (ctx->Y_spin != 0) {
+    // Y[i][Q][nu] (half-transformed vectors of this spin) is needed
+    if (ctx->Y_spin != spin) {
         s.B64_valid = false;
-        CD_RC(transform_f64(ctx, 0));
+        CD_RC(transform_f64(ctx, spin));
     }
     const double* C = s.C.as<double>();
-    const double* Gm = ctx->gam[0].as<double>();
-    // dC[nu, o+a] = 4 sum_{i,Q} Gamma[i][a][Q] Y[i][Q][nu]   (row-major [a][nu] == column-major dC)
+    const double* Gm = ctx->gam[spin].as<double>();
+    // dC[nu, o+a] = scale sum_{i,Q} Gamma[i][a][Q] Y[i][Q][nu]   (row-major [a][nu] == column-major dC)
     for (int64_t i = 0; i < o; ++i) {
         GemmF64Args g{};
         g.M = (int)v;  g.N = (int)N;  g.K = (int)M;  g.batch = 1;
         g.A = Gm + i * vp * Mp;  g.lda = Mp;  g.sA = 0;
         g.B = ctx->Y.as<double>() + i * M * N;  g.ldb = N;  g.sB = 0;
         g.C = dC + o * N;  g.ldc = N;  g.sC = 0;
-        g.alpha = 4.0;  g.beta = i == 0 ? 0.0 : 1.0;
+        g.alpha = scale;  g.beta = i == 0 ? 0.0 : 1.0;
         CD_CUDA(gemm_f64(g, true, false, ctx->stream));
         ctx->launches++;
     }
@@ -531,7 +533,7 @@ int transposed_transforms(mshqc_cd_ctx* ctx, double* dC) {
         ctx->launches++;
         ctx->Y_spin = -1;
     }
-    // dC[mu, i] = 4 sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]: only o rows, so the
+    // dC[mu, i] = scale sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]: only o rows, so the
     // long K = M*N is split over S independent partial products (batched
     // GEMM) that a deterministic reduction adds up
     {
@@ -558,7 +560,7 @@ int transposed_transforms(mshqc_cd_ctx* ctx, double* dC) {
             ctx->launches++;
         }
         sum_partials_kernel<<<(unsigned)cdiv(o * N, 256), 256, 0, ctx->stream>>>(
-            ctx->W.as<double>(), (int)S, o * N, 4.0, dC);
+            ctx->W.as<double>(), (int)S, o * N, scale, dC);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
@@ -622,108 +624,250 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
     CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 
     begin_stage(ctx, ST_TRANSPOSED);
-    CD_RC(transposed_transforms(ctx, dC));
+    CD_RC(transposed_transforms(ctx, 0, 4.0, dC));
     end_stage(ctx);
     CD_CUDA(cudaStreamSynchronize(ctx->stream));
     return MSHQC_CD_OK;
 }
 
 
-// Restricted mixed-precision gradient: exact fixed-point amplitude pass on
-// the tensor cores (writes tt as BF16 hi/lo), tensor-core Gamma GEMM with
-// round-to-nearest promotion, then the FP64 transposed transforms.
-int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
-    SpinState& s = ctx->spin[0];
-    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
-    const int64_t nblk = cdiv(v, 128), VR = nblk * 128, RQ = round_up(M, 256);
-    const int64_t KA = o * VR;
-    // transposed hi/lo copy of B: rows Q, K = (j, b)
-    const size_t nbt = (size_t)RQ * KA;
-    CD_ALLOC(ctx->BT, 2 * nbt * sizeof(uint16_t), false);
-    uint16_t* bth = ctx->BT.as<uint16_t>();
-    uint16_t* btl = bth + nbt;
-    {
-        const int64_t threads = (KA / 16) * RQ * 2;
-        const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
-        begin_stage(ctx, ST_SPLIT);
-        bt_split_kernel<<<blocks, 256, 0, ctx->stream>>>(s.B64.as<double>(), vp, Mp, (int)v, (int)M, o,
-                                                         VR, RQ, bth, btl);
-        end_stage(ctx);
-        CD_CUDA(cudaGetLastError());
-        ctx->launches++;
-    }
-    // occupied block size: FP32 integral staging S plus the BF16 hi/lo tt
-    const int64_t nby = cdiv(VR, 256), VS = nby * 256, nt = VR / 32;
+// ---------------------------------------------------------------------------
+// backward building blocks (tensor-core and FP64 unrestricted passes)
+// ---------------------------------------------------------------------------
+struct BwdDims {
+    int64_t o, v, vp;       // occupied, virtual, FP64 padding (64)
+    int64_t VR, nby, VS;    // tensor-core staging: rows per i (128), column ranges (256) per j
+};
+
+BwdDims bwd_dims(const mshqc_cd_ctx* ctx, int spin) {
+    BwdDims d;
+    d.o = ctx->spin[spin].nocc;
+    d.v = ctx->N - d.o;
+    d.vp = ctx->spin[spin].vp;
+    d.VR = cdiv(d.v, 128) * 128;
+    d.nby = cdiv(d.VR, 256);
+    d.VS = d.nby * 256;
+    return d;
+}
+
+// BF16 hi/lo copy of one spin's MO vectors transposed to rows Q (RQ rows),
+// K = (j, b) with b padded to VR: the B operand of the Gamma GEMM.
+int make_bt(mshqc_cd_ctx* ctx, int spin, DevBuf& buf, int64_t RQ, const uint16_t** hi, const uint16_t** lo) {
+    SpinState& s = ctx->spin[spin];
+    const BwdDims d = bwd_dims(ctx, spin);
+    const size_t nbt = (size_t)RQ * d.o * d.VR;
+    CD_ALLOC(buf, 2 * nbt * sizeof(uint16_t), false);
+    uint16_t* h = buf.as<uint16_t>();
+    uint16_t* l = h + nbt;
+    const int64_t threads = (d.o * d.VR / 16) * RQ * 2;
+    const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
+    begin_stage(ctx, ST_SPLIT);
+    bt_split_kernel<<<blocks, 256, 0, ctx->stream>>>(s.B64.as<double>(), s.vp, ctx->Mp, (int)d.v, (int)ctx->M,
+                                                     d.o, d.VR, RQ, h, l);
+    end_stage(ctx);
+    CD_CUDA(cudaGetLastError());
+    ctx->launches++;
+    *hi = h;
+    *lo = l;
+    return MSHQC_CD_OK;
+}
+
+// gamma[(i0 + R / VR, R % VR)][Q] (+)= sum_K A[R][K] BT[Q][K] for R < rows
+int launch_gamma(mshqc_cd_ctx* ctx, const uint16_t* ahi, const uint16_t* alo, int64_t RA, const uint16_t* bhi,
+                 const uint16_t* blo, int64_t RQ, int64_t K, int64_t rows, int64_t VR, int64_t v, int64_t vp,
+                 int i0, double* gamma, int accumulate) {
+    GammaTcArgs g{};
+    g.Ahi = ahi;  g.Alo = alo;  g.Bhi = bhi;  g.Blo = blo;
+    g.RA = RA;  g.RQ = RQ;
+    g.nk = (int)(K / 16);
+    g.KP = 32;
+    g.nrb = (int)(rows / 128);
+    g.nqb = (int)(RQ / 256);
+    g.VR = (int)VR;  g.v = (int)v;  g.vp = (int)vp;  g.Mp = (int)ctx->Mp;  g.i0 = i0;
+    g.gamma = gamma;
+    g.err = ctx->flag.as<int>() + 2;
+    g.accumulate = accumulate;
+    const size_t gsm = gamma_tc::SMEM_BYTES;
+    CD_CUDA(cudaFuncSetAttribute(gamma_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+    const int grid = (int)std::min<int64_t>((int64_t)g.nrb * g.nqb, ctx->num_sms);
+    begin_stage(ctx, ST_GAMMA);
+    gamma_tc_kernel<<<grid, gamma_tc::THREADS, gsm, ctx->stream>>>(g);
+    end_stage(ctx);
+    CD_CUDA(cudaGetLastError());
+    ctx->launches++;
+    return MSHQC_CD_OK;
+}
+
+// One mixed-precision backward pass: the occupied rows i of spin sx in
+// blocks against every j of spin sy.  Per block: (ia|jb) tiles on the tensor
+// cores (exact fixed point, FP32 staging), the element-wise amplitude pass,
+// Gamma_sx (+)= amplitudes x B_sy and, for the opposite-spin pass,
+// Gamma_sy += amplitudes^T x B_sx.  Energy partials go to `partial`
+// (ox * oy * (VRx/32) * (VRy/32) tiles).
+template <int MODE>
+int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const btx[2],
+                     const uint16_t* const bty[2], int64_t RQ, double* deps_x, double* deps_y,
+                     double* partial, int accumulate_x) {
+    SpinState& X = ctx->spin[sx];
+    SpinState& Y = ctx->spin[sy];
+    const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
+    const int64_t Mp = ctx->Mp, KA = dy.o * dy.VR;
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_i_amp = sizeof(uint16_t) * (size_t)VR * KA;
-    const size_t per_i_s = sizeof(float) * (size_t)VR * (size_t)(o * VS);
-    const size_t per_i = 2 * per_i_amp + per_i_s;
+    const size_t per_i_amp = sizeof(uint16_t) * (size_t)dx.VR * KA;
+    const size_t per_i_s = sizeof(float) * (size_t)dx.VR * (size_t)(dy.o * dy.VS);
+    const size_t per_i_t = MODE == AMP_OPPOSITE_SPIN ? per_i_amp : 0;
+    const size_t per_i = 2 * per_i_amp + per_i_s + 2 * per_i_t;
     const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 3, size_t(40) << 30));
-    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(budget / per_i)));
+    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)(budget / per_i)));
     CD_ALLOC(ctx->amp, per_i_amp * bi, false);
     CD_ALLOC(ctx->amp2, per_i_amp * bi, false);
     CD_ALLOC(ctx->W, per_i_s * bi, false);
-    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, true);
-    CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
-    CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
-    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
-    const int64_t tiles_per_i = o * nt * nt;
-    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * tiles_per_i), false);
+    if (MODE == AMP_OPPOSITE_SPIN) {
+        CD_ALLOC(ctx->ampT, per_i_t * bi, false);
+        CD_ALLOC(ctx->ampT2, per_i_t * bi, false);
+    }
+    const int64_t tiles_per_i = dy.o * (dx.VR / 32) * (dy.VR / 32);
     const size_t vsm = vtile_tc::SMEM_BYTES;
     CD_CUDA(cudaFuncSetAttribute(vtile_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
-    for (int i0 = 0; i0 < o; i0 += bi) {
-        const int nbi = (int)std::min<int64_t>(bi, o - i0);
-        // (ia|jb) for the rows i of this block and every j, each tile once
+    for (int i0 = 0; i0 < dx.o; i0 += bi) {
+        const int nbi = (int)std::min<int64_t>(bi, dx.o - i0);
         VtileArgs a{};
-        a.Xhi = s.Bhi.as<uint16_t>();  a.Xlo = s.Blo.as<uint16_t>();
-        a.ex = s.expo.as<int>();  a.diag = s.diag.as<double>();
-        a.rows = (int)s.vp16;  a.nqc = (int)(Mp / 16);
-        a.o = (int)o;  a.v = (int)v;  a.VR = (int)VR;  a.i0 = i0;  a.nbi = nbi;
-        a.nbx = (int)nblk;  a.nby = (int)nby;  a.VS = (int)VS;
+        a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
+        a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
+        a.ex = X.expo.as<int>();  a.ey = Y.expo.as<int>();
+        a.diag = sx == sy ? X.diag.as<double>() : nullptr;
+        a.rows_x = (int)X.vp16;  a.rows_y = (int)Y.vp16;
+        a.nqc = (int)(Mp / 16);
+        a.oy = (int)dy.o;  a.vx = (int)dx.v;  a.vy = (int)dy.v;
+        a.VR = (int)dx.VR;  a.i0 = i0;  a.nbi = nbi;
+        a.nbx = (int)(dx.VR / 128);  a.nby = (int)dy.nby;  a.VS = (int)dy.VS;
         a.S = ctx->W.as<float>();
         a.err = ctx->flag.as<int>();
-        const int64_t vunits = (int64_t)nbi * o * nblk * nby;
+        const int64_t vunits = (int64_t)nbi * dy.o * a.nbx * a.nby;
         const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
         begin_stage(ctx, ST_AMPLITUDE);
         vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
-        // tt = (2V - V^T)/D as BF16 hi/lo, dE/de, energy partials
         AmpElemArgs e{};
         e.S = ctx->W.as<float>();
-        e.o = (int)o;  e.v = (int)v;  e.VR = (int)VR;  e.VS = (int)VS;  e.i0 = i0;  e.nbi = nbi;
-        e.eo = s.eps.as<double>();  e.ev = e.eo + o;
+        e.ldS = dy.o * dy.VS;
+        e.rsx = (int)dx.VR;  e.csy = (int)dy.VS;  e.ksy = (int)dy.VR;
+        e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
+        e.i0 = i0;  e.nbi = nbi;
+        e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
+        e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
         e.Ahi = ctx->amp.as<uint16_t>();  e.Alo = ctx->amp2.as<uint16_t>();
-        e.RA = (long long)bi * VR;
-        e.deps = deps;
-        e.partial = ctx->partial.as<double>() + (int64_t)i0 * tiles_per_i;
-        amp_elem_kernel<<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
+        e.RA = (long long)bi * dx.VR;
+        if (MODE == AMP_OPPOSITE_SPIN) {
+            e.Thi = ctx->ampT.as<uint16_t>();  e.Tlo = ctx->ampT2.as<uint16_t>();
+            e.RT = (long long)KA;
+        }
+        e.deps_x = deps_x;  e.deps_y = deps_y;
+        e.partial = partial + (int64_t)i0 * tiles_per_i;
+        amp_elem_kernel<MODE, true><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
         end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
-        GammaTcArgs g{};
-        g.Ahi = ctx->amp.as<uint16_t>();  g.Alo = ctx->amp2.as<uint16_t>();
-        g.Bhi = bth;  g.Blo = btl;
-        g.RA = (long long)bi * VR;  g.RQ = RQ;
-        g.nk = (int)(KA / 16);
-        g.KP = 32;
-        g.nrb = (int)(nbi * VR / 128);
-        g.nqb = (int)(RQ / 256);
-        g.VR = (int)VR;  g.v = (int)v;  g.vp = (int)vp;  g.Mp = (int)Mp;  g.i0 = i0;
-        g.gamma = ctx->gam[0].as<double>();
-        g.err = ctx->flag.as<int>() + 2;
-        const size_t gsm = gamma_tc::SMEM_BYTES;
-        CD_CUDA(cudaFuncSetAttribute(gamma_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
-        const int ggrid = (int)std::min<int64_t>((int64_t)g.nrb * g.nqb, ctx->num_sms);
-        begin_stage(ctx, ST_GAMMA);
-        gamma_tc_kernel<<<ggrid, gamma_tc::THREADS, gsm, ctx->stream>>>(g);
-        end_stage(ctx);
-        CD_CUDA(cudaGetLastError());
-        ctx->launches++;
+        CD_RC(launch_gamma(ctx, e.Ahi, e.Alo, e.RA, bty[0], bty[1], RQ, KA, (int64_t)nbi * dx.VR, dx.VR, dx.v,
+                           dx.vp, i0, ctx->gam[sx].as<double>(), accumulate_x));
+        if (MODE == AMP_OPPOSITE_SPIN) {
+            // K range of this block inside the transposed B of spin sx
+            const size_t k0 = (size_t)i0 * dx.VR * RQ;
+            CD_RC(launch_gamma(ctx, e.Thi, e.Tlo, KA, btx[0] + k0, btx[1] + k0, RQ, (int64_t)nbi * dx.VR, KA,
+                               dy.VR, dy.v, dy.vp, 0, ctx->gam[sy].as<double>(), 1));
+        }
     }
-    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * tiles_per_i),
-                                                   ctx->totals.as<double>());
+    return MSHQC_CD_OK;
+}
+
+// The FP64 counterpart: S = B_x(block) B_y^T and the Gamma products as FP64
+// DMMA GEMMs around the same element-wise pass.
+template <int MODE>
+int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double* deps_y, double* partial) {
+    SpinState& X = ctx->spin[sx];
+    SpinState& Y = ctx->spin[sy];
+    const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
+    const int64_t Mp = ctx->Mp, ldS = dy.o * dy.vp;
+    size_t free_b = 0, total_b = 0;
+    CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_i = 2 * sizeof(double) * (size_t)dx.vp * ldS;
+    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 4, size_t(32) << 30));
+    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)(budget / per_i)));
+    CD_ALLOC(ctx->W, per_i / 2 * bi, false);
+    CD_ALLOC(ctx->amp, per_i / 2 * bi, false);
+    const int64_t tiles_per_i = dy.o * (dx.vp / 32) * (dy.vp / 32);
+    for (int i0 = 0; i0 < dx.o; i0 += bi) {
+        const int nbi = (int)std::min<int64_t>(bi, dx.o - i0);
+        const double* Xb = X.B64.as<double>() + (int64_t)i0 * dx.vp * Mp;
+        // S[(i,a)][(j,b)] = sum_Q X[(i,a)][Q] Y[(j,b)][Q]
+        GemmF64Args g{};
+        g.M = (int)(nbi * dx.vp);  g.N = (int)ldS;  g.K = (int)Mp;  g.batch = 1;
+        g.A = Xb;  g.lda = Mp;  g.sA = 0;
+        g.B = Y.B64.as<double>();  g.ldb = Mp;  g.sB = 0;
+        g.C = ctx->W.as<double>();  g.ldc = ldS;  g.sC = 0;
+        g.alpha = 1.0;  g.beta = 0.0;
+        begin_stage(ctx, ST_AMPLITUDE);
+        CD_CUDA(gemm_f64(g, true, true, ctx->stream));
+        ctx->launches++;
+        AmpElemArgs e{};
+        e.S = ctx->W.as<double>();
+        e.ldS = ldS;
+        e.rsx = (int)dx.vp;  e.csy = (int)dy.vp;  e.ksy = (int)dy.vp;
+        e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
+        e.i0 = i0;  e.nbi = nbi;
+        e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
+        e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
+        e.A64 = ctx->amp.as<double>();  e.ldA = ldS;
+        e.deps_x = deps_x;  e.deps_y = deps_y;
+        e.partial = partial + (int64_t)i0 * tiles_per_i;
+        amp_elem_kernel<MODE, false><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
+        end_stage(ctx);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+        begin_stage(ctx, ST_GAMMA);
+        // Gamma_x[(i,a)][Q] += sum_{(j,b)} t[(i,a)][(j,b)] Y[(j,b)][Q]
+        GemmF64Args h{};
+        h.M = (int)(nbi * dx.vp);  h.N = (int)Mp;  h.K = (int)ldS;  h.batch = 1;
+        h.A = ctx->amp.as<double>();  h.lda = ldS;  h.sA = 0;
+        h.B = Y.B64.as<double>();  h.ldb = Mp;  h.sB = 0;
+        h.C = ctx->gam[sx].as<double>() + (int64_t)i0 * dx.vp * Mp;  h.ldc = Mp;  h.sC = 0;
+        h.alpha = 1.0;  h.beta = 1.0;
+        CD_CUDA(gemm_f64(h, true, false, ctx->stream));
+        ctx->launches++;
+        if (MODE == AMP_OPPOSITE_SPIN) {
+            // Gamma_y[(j,b)][Q] += sum_{(i,a) in block} t[(i,a)][(j,b)] X[(i,a)][Q]
+            GemmF64Args k{};
+            k.M = (int)ldS;  k.N = (int)Mp;  k.K = (int)(nbi * dx.vp);  k.batch = 1;
+            k.A = ctx->amp.as<double>();  k.lda = ldS;  k.sA = 0;
+            k.B = Xb;  k.ldb = Mp;  k.sB = 0;
+            k.C = ctx->gam[sy].as<double>();  k.ldc = Mp;  k.sC = 0;
+            k.alpha = 1.0;  k.beta = 1.0;
+            CD_CUDA(gemm_f64(k, false, false, ctx->stream));
+            ctx->launches++;
+        }
+        end_stage(ctx);
+    }
+    return MSHQC_CD_OK;
+}
+
+// Restricted mixed-precision gradient: one tensor-core pass, then the FP64
+// transposed transforms with dE/dB = 4 Gamma.
+int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
+    SpinState& s = ctx->spin[0];
+    const BwdDims d = bwd_dims(ctx, 0);
+    const int64_t N = ctx->N, Mp = ctx->Mp, RQ = round_up(ctx->M, 256);
+    const uint16_t* bt[2] = {nullptr, nullptr};
+    CD_RC(make_bt(ctx, 0, ctx->BT, RQ, &bt[0], &bt[1]));
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)d.o * s.vp * Mp, true);
+    CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
+    CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+    const int64_t tiles = d.o * d.o * (d.VR / 32) * (d.VR / 32);
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)tiles, false);
+    CD_RC(tc_backward_pass<AMP_RESTRICTED>(ctx, 0, 0, bt, bt, RQ, deps, deps, ctx->partial.as<double>(), 0));
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)tiles, ctx->totals.as<double>());
     CD_CUDA(cudaGetLastError());
     ctx->launches++;
     int herr[4] = {0, 0, 0, 0};
@@ -735,7 +879,61 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
                                                    std::to_string(herr[0] ? herr[0] : herr[2]) + ")");
     if (herr[1]) ctx->fixed_point_exact = 0;
     begin_stage(ctx, ST_TRANSPOSED);
-    CD_RC(transposed_transforms(ctx, dC));
+    CD_RC(transposed_transforms(ctx, 0, 4.0, dC));
+    end_stage(ctx);
+    return MSHQC_CD_OK;
+}
+
+// Unrestricted gradient (CD-UMP2 energy, the OMP2 step): same-spin passes for
+// alpha and beta and one opposite-spin pass, Gamma accumulated per spin, then
+// the transposed transforms of each spin with dE/dB = 2 Gamma.  e3 receives
+// ss_aa, ss_bb, os.
+int gradient_unrestricted(mshqc_cd_ctx* ctx, int precision, double* const dC[2], double* const deps[2],
+                          double* e3) {
+    const BwdDims da = bwd_dims(ctx, 0), db = bwd_dims(ctx, 1);
+    const int64_t N = ctx->N, Mp = ctx->Mp, RQ = round_up(ctx->M, 256);
+    const bool tc = precision == MSHQC_CD_FP16X3;
+    const uint16_t* bta[2] = {nullptr, nullptr};
+    const uint16_t* btb[2] = {nullptr, nullptr};
+    if (tc) {
+        CD_RC(make_bt(ctx, 0, ctx->BT, RQ, &bta[0], &bta[1]));
+        CD_RC(make_bt(ctx, 1, ctx->BT_b, RQ, &btb[0], &btb[1]));
+    }
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)da.o * da.vp * Mp, true);
+    CD_ALLOC(ctx->gam[1], sizeof(double) * (size_t)db.o * db.vp * Mp, true);
+    for (int s = 0; s < 2; ++s) CD_CUDA(cudaMemsetAsync(deps[s], 0, sizeof(double) * N, ctx->stream));
+    CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+    const int64_t ra = tc ? da.VR / 32 : da.vp / 32, rb = tc ? db.VR / 32 : db.vp / 32;
+    const int64_t n0 = da.o * da.o * ra * ra, n1 = db.o * db.o * rb * rb, n2 = da.o * db.o * ra * rb;
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(n0 + n1 + n2), false);
+    double* part = ctx->partial.as<double>();
+    if (tc) {
+        CD_RC(tc_backward_pass<AMP_SAME_SPIN>(ctx, 0, 0, bta, bta, RQ, deps[0], deps[0], part, 1));
+        CD_RC(tc_backward_pass<AMP_SAME_SPIN>(ctx, 1, 1, btb, btb, RQ, deps[1], deps[1], part + n0, 1));
+        CD_RC(tc_backward_pass<AMP_OPPOSITE_SPIN>(ctx, 0, 1, bta, btb, RQ, deps[0], deps[1], part + n0 + n1, 1));
+    } else {
+        CD_RC(f64_backward_pass<AMP_SAME_SPIN>(ctx, 0, 0, deps[0], deps[0], part));
+        CD_RC(f64_backward_pass<AMP_SAME_SPIN>(ctx, 1, 1, deps[1], deps[1], part + n0));
+        CD_RC(f64_backward_pass<AMP_OPPOSITE_SPIN>(ctx, 0, 1, deps[0], deps[1], part + n0 + n1));
+    }
+    const int64_t offs[3] = {0, n0, n0 + n1}, cnt[3] = {n0, n1, n2};
+    for (int k = 0; k < 3; ++k) {
+        reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(part + offs[k], (int)cnt[k], ctx->totals.as<double>() + k);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+    }
+    int herr[4] = {0, 0, 0, 0};
+    CD_CUDA(cudaMemcpyAsync(herr, ctx->flag.p, sizeof(herr), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaMemcpyAsync(e3, ctx->totals.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (herr[0] || herr[2])
+        return set_error(MSHQC_CD_ERR_TIMEOUT, "tensor-core backward gave up waiting (site " +
+                                                   std::to_string(herr[0] ? herr[0] : herr[2]) + ")");
+    if (herr[1]) ctx->fixed_point_exact = 0;
+    begin_stage(ctx, ST_TRANSPOSED);
+    CD_RC(transposed_transforms(ctx, 0, 2.0, dC[0]));
+    CD_RC(transposed_transforms(ctx, 1, 2.0, dC[1]));
     end_stage(ctx);
     return MSHQC_CD_OK;
 }
@@ -744,32 +942,47 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
 
 int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out, double* dC_a,
                  double* dC_b, double* deps_a, double* deps_b, int where) {
-    if (kind != MSHQC_CD_RESTRICTED)
-        return set_error(MSHQC_CD_ERR_UNSUPPORTED, "unrestricted gradient not built yet");
-    (void)dC_b;
-    (void)deps_b;
+    if (kind != MSHQC_CD_RESTRICTED && kind != MSHQC_CD_UNRESTRICTED)
+        return set_error(MSHQC_CD_ERR_ARG, "unknown kind");
+    const bool unres = kind == MSHQC_CD_UNRESTRICTED;
     CD_RC(require_inputs(ctx, 0));
+    if (unres) CD_RC(require_inputs(ctx, 1));
     const int64_t N = ctx->N;
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     reset_stages(ctx);
     CD_CUDA(cudaEventRecord(e0, ctx->stream));
     CD_RC(ensure_transform(ctx, 0, precision));
+    if (unres) CD_RC(ensure_transform(ctx, 1, precision));
     CD_CUDA(cudaEventRecord(e1, ctx->stream));
-    CD_ALLOC(ctx->grad[0], sizeof(double) * (size_t)(N * N + N), false);
-    double* dC = ctx->grad[0].as<double>();
-    double* de = dC + N * N;
+    double* dC[2] = {nullptr, nullptr};
+    double* de[2] = {nullptr, nullptr};
+    for (int s = 0; s < (unres ? 2 : 1); ++s) {
+        CD_ALLOC(ctx->grad[s], sizeof(double) * (size_t)(N * N + N), false);
+        dC[s] = ctx->grad[s].as<double>();
+        de[s] = dC[s] + N * N;
+    }
+    double e3[3] = {0.0, 0.0, 0.0};
     double energy = 0.0;
     ctx->fixed_point_exact = 1;
-    if (precision == MSHQC_CD_FP64)
-        CD_RC(gradient_restricted_f64(ctx, dC, de, &energy));
-    else
-        CD_RC(gradient_restricted_tc(ctx, dC, de, &energy));
+    if (unres) {
+        CD_RC(gradient_unrestricted(ctx, precision, dC, de, e3));
+        energy = e3[0] + e3[1] + e3[2];
+    } else if (precision == MSHQC_CD_FP64) {
+        CD_RC(gradient_restricted_f64(ctx, dC[0], de[0], &energy));
+    } else {
+        CD_RC(gradient_restricted_tc(ctx, dC[0], de[0], &energy));
+    }
     CD_CUDA(cudaEventRecord(e2, ctx->stream));
     CD_CUDA(cudaEventSynchronize(e2));
     collect_stages(ctx);
     if (e_out) {
         std::memset(e_out, 0, sizeof(*e_out));
         e_out->total = energy;
+        if (unres) {
+            e_out->ss_aa = e3[0];
+            e_out->ss_bb = e3[1];
+            e_out->os = e3[2];
+        }
         float t01 = 0, t12 = 0;
         CD_CUDA(cudaEventElapsedTime(&t01, e0, e1));
         CD_CUDA(cudaEventElapsedTime(&t12, e1, e2));
@@ -777,8 +990,12 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
         e_out->ms_energy = t12;
         e_out->ms_total = t01 + t12;
     }
-    CD_RC(download(ctx, dC_a, dC, sizeof(double) * N * N, where));
-    CD_RC(download(ctx, deps_a, de, sizeof(double) * N, where));
+    CD_RC(download(ctx, dC_a, dC[0], sizeof(double) * N * N, where));
+    CD_RC(download(ctx, deps_a, de[0], sizeof(double) * N, where));
+    if (unres) {
+        CD_RC(download(ctx, dC_b, dC[1], sizeof(double) * N * N, where));
+        CD_RC(download(ctx, deps_b, de[1], sizeof(double) * N, where));
+    }
     return MSHQC_CD_OK;
 }
 

@@ -2,10 +2,10 @@
 //
 //   Gamma[(i,a)][Q] = sum_{(j,b)} tt[(i,a)][(j,b)] B[(j,b)][Q]
 //
-// A operand: the amplitude staging matrix written by the AMPLITUDE mode of the
-// pair kernel (rows (i - i0, a), K = (j, b)); B operand: BT, the MO vectors
-// transposed to rows Q, K = (j, b).  Both are BF16 hi/lo pairs in the blocked
-// K-major layout of pair_energy_tc.cuh (element (r, k) of a matrix with R rows
+// A operand: the amplitude operand written by amp_elem.cuh (rows (i - i0, a),
+// K = (j, b)); B operand: BT, the MO vectors transposed to rows Q, K = (j, b).
+// Both are BF16 hi/lo pairs in the blocked K-major layout of pair_energy_tc.cuh
+// (element (r, k) of a matrix with R rows
 // at (k/16)*R*16 + (r/8*16 + (k%16)/8*8 + r%8)*8 + k%8).
 //
 // Tile 128 rows x 256 Q; per 16-wide K step three 128x256x16 MMAs
@@ -36,6 +36,7 @@ struct GammaTcArgs {
     int nrb, nqb;           // row blocks (of 128) and Q blocks (of 256) to compute
     int VR, v, vp, Mp, i0;  // output mapping R -> (i0 + R / VR, R % VR)
     double* gamma;          // [o][vp][Mp]
+    int accumulate;         // 1: gamma += result, 0: gamma = result
     int* err;
 };
 
@@ -211,9 +212,15 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
             if (a < p.v) {
                 double* dst = p.gamma + ((long long)i * p.vp + a) * p.Mp;
                 const int q0 = (int)(qb * BN) + part * 64;
+                if (p.accumulate) {
 #pragma unroll
-                for (int c = 0; c < 64; ++c)
-                    if (q0 + c < p.Mp) dst[q0 + c] = (double)acc[c];
+                    for (int c = 0; c < 64; ++c)
+                        if (q0 + c < p.Mp) dst[q0 + c] += (double)acc[c];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 64; ++c)
+                        if (q0 + c < p.Mp) dst[q0 + c] = (double)acc[c];
+                }
             }
         }
     }

@@ -86,3 +86,95 @@ def test_restricted_mixed_gradient_vs_oracle(ctx):
     assert abs(g.energy["total"] - ref["E"]) <= 1e-6
     assert np.max(np.abs(g.dC_a - ref["dC"])) <= 1e-6
     assert np.max(np.abs(g.deps_a - ref["deps"])) <= 1e-6
+
+
+# ---------------------------------------------------------------------------
+# Unrestricted (CD-UMP2 energy, the OMP2 step): dE/dC and dE/deps per spin.
+# ---------------------------------------------------------------------------
+def set_unrestricted(ctx, inp):
+    A, B = inp.alpha, inp.beta
+    ctx.set_vectors(inp.L)
+    ctx.set_orbitals(capi.ALPHA, A.C, A.eps, A.nocc)
+    ctx.set_orbitals(capi.BETA, B.C, B.eps, B.nocc)
+
+
+def maxrel(x, ref):
+    return np.max(np.abs(x - ref)) / np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("N,oa,ob,M,seed", [(26, 6, 5, 70, 1), (45, 7, 4, 101, 2), (80, 9, 8, 190, 3)])
+def test_unrestricted_fp64_gradient_vs_oracle(ctx, N, oa, ob, M, seed):
+    inp = syn.make_inputs(N, oa, M, seed=seed, nocc_beta=ob)
+    A, B = inp.alpha, inp.beta
+    ref = orc.unrestricted_gradient(inp.L, A.C, B.C, A.eps, B.eps, oa, ob)
+    set_unrestricted(ctx, inp)
+    g = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP64)
+    for key in ("ss_aa", "ss_bb", "os"):
+        assert abs(g.energy[key] - ref[key]) <= 1e-12 * abs(ref[key]), key
+    assert abs(g.energy["total"] - ref["E"]) <= 1e-12 * abs(ref["E"])
+    assert maxrel(g.dC_a, ref["dC_a"]) <= 1e-10
+    assert maxrel(g.dC_b, ref["dC_b"]) <= 1e-10
+    assert maxrel(g.deps_a, ref["deps_a"]) <= 1e-10
+    assert maxrel(g.deps_b, ref["deps_b"]) <= 1e-10
+
+
+def test_unrestricted_energy_matches_energy_entry(ctx):
+    inp = twin(64, 8, 160, seed=5, nocc_beta=6)
+    set_unrestricted(ctx, inp)
+    e = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP64)
+    g = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP64)
+    for key in ("ss_aa", "ss_bb", "os", "total"):
+        assert abs(g.energy[key] - e[key]) <= 1e-12 * abs(e[key]) + 1e-15, key
+
+
+def test_unrestricted_closed_shell_limit(ctx):
+    """C_a = C_b, equal occupations: dE/dC_a + dE/dC_b equals the restricted
+    dE/dC (FP64 and mixed)."""
+    N, o, M = 70, 8, 170
+    inp = twin(N, o, M, seed=9)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    r = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
+    ctx.set_orbitals(capi.BETA, a.C, a.eps, o)
+    for prec, tol in ((capi.FP64, 1e-10), (capi.FP16X3, 1e-6)):
+        u = ctx.mp2_gradient(capi.UNRESTRICTED, prec)
+        scale = 1.0 if prec == capi.FP16X3 else np.max(np.abs(r.dC_a))
+        assert abs(u.energy["total"] - r.energy["total"]) <= (1e-12 if prec == capi.FP64 else 1e-6)
+        assert np.max(np.abs(u.dC_a + u.dC_b - r.dC_a)) <= tol * scale
+        assert np.max(np.abs(u.deps_a + u.deps_b - r.deps_a)) <= tol * (1.0 if prec == capi.FP16X3
+                                                                          else np.max(np.abs(r.deps_a)))
+
+
+def test_unrestricted_orbital_gradient_fd(ctx):
+    """g_ai of each spin from the GPU dE/dC against central differences of the
+    GPU UMP2 energy under C_s -> C_s exp(-h K) (step 1e-4)."""
+    N, oa, ob, M = 40, 6, 4, 100
+    inp = twin(N, oa, M, seed=11, nocc_beta=ob)
+    A, B = inp.alpha, inp.beta
+    set_unrestricted(ctx, inp)
+    g = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP64)
+    h = 1e-4
+    for spin, S, o, dC in ((capi.ALPHA, A, oa, g.dC_a), (capi.BETA, B, ob, g.dC_b)):
+        kg = orc.orbital_gradient(S.C, dC, o)
+        for (ai, ii) in [(0, 0), (5, o - 1), (20, 1)]:
+            K = np.zeros((N, N))
+            K[o + ai, ii], K[ii, o + ai] = 1.0, -1.0
+            ctx.set_orbitals(spin, S.C @ scipy.linalg.expm(-h * K), S.eps, o)
+            ep = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP64)["total"]
+            ctx.set_orbitals(spin, S.C @ scipy.linalg.expm(h * K), S.eps, o)
+            em = ctx.mp2_energy(capi.UNRESTRICTED, capi.FP64)["total"]
+            ctx.set_orbitals(spin, S.C, S.eps, o)
+            fd = (ep - em) / (2 * h)
+            assert abs(fd - kg[ai, ii]) <= 1e-6, (spin, ai, ii, fd, kg[ai, ii])
+
+
+@pytest.mark.parametrize("N,oa,ob,M,seed", [(60, 8, 7, 150, 3), (131, 14, 11, 300, 5), (210, 19, 17, 520, 6)])
+def test_unrestricted_mixed_gradient_vs_fp64(ctx, N, oa, ob, M, seed):
+    inp = twin(N, oa, M, seed=seed, nocc_beta=ob)
+    set_unrestricted(ctx, inp)
+    g64 = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP64)
+    g3 = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP16X3)
+    for key in ("ss_aa", "ss_bb", "os", "total"):
+        assert abs(g3.energy[key] - g64.energy[key]) <= 1e-6, key
+    for x, y in ((g3.dC_a, g64.dC_a), (g3.dC_b, g64.dC_b), (g3.deps_a, g64.deps_a), (g3.deps_b, g64.deps_b)):
+        assert np.max(np.abs(x - y)) <= 1e-6, np.max(np.abs(x - y))
