@@ -149,6 +149,58 @@ MSHQC_CD_API int mshqc_cd_mp2_gradient(mshqc_cd_ctx* ctx, int kind, int precisio
                           mshqc_cd_energy* e_out, double* dC_a, double* dC_b,
                           double* deps_a, double* deps_b, int where);
 
+/* --- CD-OMP2 (FP64; reference src/mp2/cholesky_omp2.cc) ---------------- */
+/* Core Hamiltonian H (N*N, symmetric) of the OMP2 generalized Fock matrix:
+ * IntegralEngine::compute_core_hamiltonian as read by
+ * CholeskyOMP2::build_gfock_from_density (src/mp2/cholesky_omp2.cc:336). */
+MSHQC_CD_API int mshqc_cd_set_core_hamiltonian(mshqc_cd_ctx* ctx, const double* H, int where);
+
+/* Current orbitals of one spin (N*N column-major); after mshqc_cd_omp2 these
+ * are the rotated orbitals (OMP2Result::C_alpha / C_beta). */
+MSHQC_CD_API int mshqc_cd_get_orbitals(mshqc_cd_ctx* ctx, int spin, double* C, int where);
+
+/* One gradient evaluation of CholeskyOMP2::compute at the context's current
+ * alpha and beta orbitals (src/mp2/cholesky_omp2.cc:442-466): amplitudes
+ * (:94-183), MP2 energy (:189-230), the one-particle density blocks G_oo
+ * (o*o) and G_vv (v*v) per spin (:232-326, row-major), and the generalized
+ * Fock matrices F = C^T (H + J - K) C (:331-369, N*N column-major); the
+ * reference gradient is w_ai = 2 F(o+a, i) (:465-466).  P_a / P_b: the
+ * reference densities SCFResult::P_alpha / P_beta (N*N), or NULL for
+ * C_occ C_occ^T.  Any output may be NULL.  Both spins must be set (the same
+ * orbitals twice for a closed shell) and the core Hamiltonian given. */
+MSHQC_CD_API int mshqc_cd_omp2_pieces(mshqc_cd_ctx* ctx, const double* P_a, const double* P_b,
+                                      double* e_mp2, double* Goo_a, double* Gvv_a, double* Goo_b,
+                                      double* Gvv_b, double* F_a, double* F_b, int where);
+
+/* CholeskyOMP2Config (reference include/mshqc/cholesky_omp2.h:28-34) plus
+ * the SCF energy the reference reads from SCFResult::energy_total. */
+typedef struct {
+    int max_iterations;        /* 50 */
+    double energy_threshold;   /* 1e-6 */
+    double gradient_threshold; /* 1e-5 */
+    double e_scf;
+} mshqc_cd_omp2_config;
+
+/* The energies and counters of OMP2Result (reference include/mshqc/mp2.h:52-72). */
+typedef struct {
+    double energy_scf;
+    double energy_mp2_corr;
+    double energy_total;       /* E_SCF + E_MP2 of the last iteration before the final one */
+    int iterations;
+    int converged;
+    double ms_total;
+} mshqc_cd_omp2_result;
+
+/* CholeskyOMP2::compute (src/mp2/cholesky_omp2.cc:427-512): repeat the
+ * gradient evaluation, stop when |w| < gradient_threshold and |dE| <
+ * energy_threshold, else rotate C <- C exp(-kappa) with kappa_ai =
+ * 0.5 w_ai / (F_aa - F_ii + 0.2) (|denominator| >= 1e-2; :375-424); when
+ * nocc_alpha == nocc_beta beta takes alpha's orbitals after each step.
+ * Orbital energies and E_SCF are never updated, as in the reference.  The
+ * final orbitals replace the context's (mshqc_cd_get_orbitals). */
+MSHQC_CD_API int mshqc_cd_omp2(mshqc_cd_ctx* ctx, const mshqc_cd_omp2_config* cfg, const double* P_a,
+                               const double* P_b, int where, mshqc_cd_omp2_result* res);
+
 /* --- allocation-free energy (no counterpart in the reference) --------- */
 /* Size of the static device scratch of mshqc_cd_rmp2_energy_noalloc. */
 #define MSHQC_CD_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmshqc_cuda.so")
 
-CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_noalloc.cu"]
+CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_omp2.cu", "cd_noalloc.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

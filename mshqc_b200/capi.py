@@ -34,6 +34,17 @@ class CDError(RuntimeError):
         self.code = code
 
 
+class Omp2Config(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int), ("energy_threshold", ctypes.c_double),
+                ("gradient_threshold", ctypes.c_double), ("e_scf", ctypes.c_double)]
+
+
+class Omp2Result(ctypes.Structure):
+    _fields_ = [("energy_scf", ctypes.c_double), ("energy_mp2_corr", ctypes.c_double),
+                ("energy_total", ctypes.c_double), ("iterations", ctypes.c_int),
+                ("converged", ctypes.c_int), ("ms_total", ctypes.c_double)]
+
+
 class Energy(ctypes.Structure):
     _fields_ = [("ss_aa", ctypes.c_double), ("ss_bb", ctypes.c_double),
                 ("os", ctypes.c_double), ("total", ctypes.c_double),
@@ -65,6 +76,11 @@ SIGNATURES = {
     "mshqc_cd_pair_energies": (_i32, [_vp, _i32, _vp, _i32]),
     "mshqc_cd_mp2_gradient": (_i32, [_vp, _i32, _i32, ctypes.POINTER(Energy), _vp, _vp, _vp,
                                      _vp, _i32]),
+    "mshqc_cd_set_core_hamiltonian": (_i32, [_vp, _vp, _i32]),
+    "mshqc_cd_get_orbitals": (_i32, [_vp, _i32, _vp, _i32]),
+    "mshqc_cd_omp2_pieces": (_i32, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double), _vp, _vp, _vp, _vp,
+                                    _vp, _vp, _i32]),
+    "mshqc_cd_omp2": (_i32, [_vp, ctypes.POINTER(Omp2Config), _vp, _vp, _i32, ctypes.POINTER(Omp2Result)]),
     "mshqc_cd_rmp2_energy_noalloc": (_i32, [_vp, _vp, _i64, _i64, _i64, _vp, _vp]),
 }
 
@@ -247,6 +263,55 @@ class Context:
             _ptr(dCb) if dCb is not None else None, _ptr(dea),
             _ptr(deb) if deb is not None else None, HOST))
         return Gradient(e.as_dict(), dCa, dCb, dea, deb)
+
+    # -- CD-OMP2 ------------------------------------------------------------
+    def set_core_hamiltonian(self, H):
+        """Core Hamiltonian (N x N, symmetric) of the OMP2 generalized Fock."""
+        Hc = _host_f64(H)
+        _check(self._lib.mshqc_cd_set_core_hamiltonian(self._h, _ptr(Hc), HOST))
+        return self
+
+    def get_orbitals(self, spin: int = ALPHA) -> np.ndarray:
+        N = self.nbf
+        C = np.empty((N, N), dtype=np.float64, order="F")
+        _check(self._lib.mshqc_cd_get_orbitals(self._h, spin, _ptr(C), HOST))
+        return C
+
+    def _densities(self, P_a, P_b):
+        pa = _host_f64(P_a, "F") if P_a is not None else None
+        pb = _host_f64(P_b, "F") if P_b is not None else None
+        return pa, pb, (_ptr(pa) if pa is not None else None), (_ptr(pb) if pb is not None else None)
+
+    def omp2_pieces(self, P_a=None, P_b=None) -> dict:
+        """One CholeskyOMP2 gradient evaluation: e_mp2, G_oo / G_vv per spin,
+        F_mo per spin (N x N) and w_ai = 2 F(o+a, i)."""
+        N = self.nbf
+        oa, ob = self.nocc
+        out = {"Goo_a": np.empty((oa, oa)), "Gvv_a": np.empty((N - oa, N - oa)),
+               "Goo_b": np.empty((ob, ob)), "Gvv_b": np.empty((N - ob, N - ob)),
+               "F_a": np.empty((N, N), order="F"), "F_b": np.empty((N, N), order="F")}
+        e = ctypes.c_double()
+        pa, pb, ppa, ppb = self._densities(P_a, P_b)
+        _check(self._lib.mshqc_cd_omp2_pieces(
+            self._h, ppa, ppb, ctypes.byref(e), _ptr(out["Goo_a"]), _ptr(out["Gvv_a"]),
+            _ptr(out["Goo_b"]), _ptr(out["Gvv_b"]), _ptr(out["F_a"]), _ptr(out["F_b"]), HOST))
+        out["e_mp2"] = e.value
+        out["w_a"] = 2.0 * out["F_a"][oa:, :oa]
+        out["w_b"] = 2.0 * out["F_b"][ob:, :ob]
+        return out
+
+    def omp2(self, max_iterations: int = 50, energy_threshold: float = 1e-6,
+             gradient_threshold: float = 1e-5, e_scf: float = 0.0, P_a=None, P_b=None) -> dict:
+        """CholeskyOMP2::compute; the rotated orbitals stay in the context."""
+        cfg = Omp2Config(int(max_iterations), float(energy_threshold), float(gradient_threshold),
+                         float(e_scf))
+        res = Omp2Result()
+        pa, pb, ppa, ppb = self._densities(P_a, P_b)
+        _check(self._lib.mshqc_cd_omp2(self._h, ctypes.byref(cfg), ppa, ppb, HOST, ctypes.byref(res)))
+        return {"energy_scf": res.energy_scf, "energy_mp2_corr": res.energy_mp2_corr,
+                "energy_total": res.energy_total, "iterations": res.iterations,
+                "converged": bool(res.converged), "ms_total": res.ms_total,
+                "C_alpha": self.get_orbitals(ALPHA), "C_beta": self.get_orbitals(BETA)}
 
 
 def noalloc_shape(nocc: int, nvir: int, nvec: int) -> tuple[int, int, int]:

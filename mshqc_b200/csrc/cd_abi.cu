@@ -107,20 +107,6 @@ DeviceGuard::~DeviceGuard() {
 }
 }  // namespace mshqc_cd
 
-#define CD_CUDA(call)                                                     \
-    do {                                                                  \
-        cudaError_t _e = (call);                                          \
-        if (_e != cudaSuccess) return cuda_error(_e, #call);              \
-    } while (0)
-#define CD_ALLOC(buf, nbytes, zero)                                                        \
-    do {                                                                                   \
-        cudaError_t _e = (buf).reserve((nbytes), (zero), ctx->stream);                     \
-        if (_e == cudaErrorMemoryAllocation)                                               \
-            return set_error(MSHQC_CD_ERR_ALLOC, "device allocation of " +                 \
-                                                     std::to_string((size_t)(nbytes)) +    \
-                                                     " bytes failed");                     \
-        if (_e != cudaSuccess) return cuda_error(_e, "workspace");                         \
-    } while (0)
 #define CD_CHECK_CTX()                                                                  \
     do {                                                                                \
         if (!ctx) return set_error(MSHQC_CD_ERR_ARG, "null context");                   \

@@ -90,6 +90,11 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf W;             // backward: integral staging / C_vir-contracted Gamma
     mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
     mshqc_cd::DevBuf diag_os;       // sum_Q B_alpha[i][a] B_beta[i][a] (opposite-spin diagonal)
+    mshqc_cd::DevBuf Hcore;         // OMP2: core Hamiltonian N*N
+    bool H_set = false;
+    mshqc_cd::DevBuf opdm;          // OMP2: OPDM blocks, densities, Fock matrices
+    mshqc_cd::DevBuf omp2_ws;       // OMP2: split-K partials, rotation work matrices
+    mshqc_cd::DevBuf Zt;            // OMP2: P L^Q for every Q (M*N*N)
     bool diag_os_valid = false;
     int fixed_point_exact = 1;      // Cauchy-Schwarz bound of the last tensor-core pass held
 
@@ -143,6 +148,10 @@ struct mshqc_cd_ctx {
             s.norms.release();
         }
         diag_os.release();
+        Hcore.release();
+        opdm.release();
+        omp2_ws.release();
+        Zt.release();
         for (auto& g : gam) g.release();
         for (auto& g : grad) g.release();
     }
@@ -162,9 +171,32 @@ int upload(mshqc_cd_ctx* ctx, void* dst, const void* src, size_t nbytes);
 int download(mshqc_cd_ctx* ctx, void* dst, const void* src, size_t nbytes, int where);
 int check_finite_device(mshqc_cd_ctx* ctx, const double* x, int64_t n, const char* what);
 
+// status helpers for functions returning an MSHQC_CD_* code (CD_ALLOC needs
+// a `ctx` in scope)
+#define CD_CUDA(call)                                                     \
+    do {                                                                  \
+        cudaError_t _e = (call);                                          \
+        if (_e != cudaSuccess) return cuda_error(_e, #call);              \
+    } while (0)
+#define CD_ALLOC(buf, nbytes, zero)                                                        \
+    do {                                                                                   \
+        cudaError_t _e = (buf).reserve((nbytes), (zero), ctx->stream);                     \
+        if (_e == cudaErrorMemoryAllocation)                                               \
+            return set_error(MSHQC_CD_ERR_ALLOC, "device allocation of " +                 \
+                                                     std::to_string((size_t)(nbytes)) +    \
+                                                     " bytes failed");                     \
+        if (_e != cudaSuccess) return cuda_error(_e, "workspace");                         \
+    } while (0)
+#define CD_RC(x)             \
+    do {                     \
+        int _rc = (x);       \
+        if (_rc) return _rc; \
+    } while (0)
+
 // implemented in cd_mp2.cu
 int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision);
 int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out);
 int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out,
                  double* dC_a, double* dC_b, double* deps_a, double* deps_b, int where);
+int invalidate_spin(mshqc_cd_ctx* ctx, int spin);   // orbitals of `spin` changed on the device
 }  // namespace mshqc_cd

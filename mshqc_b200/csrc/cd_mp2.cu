@@ -21,25 +21,6 @@
 
 namespace mshqc_cd {
 
-#define CD_CUDA(call)                                                     \
-    do {                                                                  \
-        cudaError_t _e = (call);                                          \
-        if (_e != cudaSuccess) return cuda_error(_e, #call);              \
-    } while (0)
-#define CD_ALLOC(buf, nbytes, zero)                                                        \
-    do {                                                                                   \
-        cudaError_t _e = (buf).reserve((nbytes), (zero), ctx->stream);                     \
-        if (_e == cudaErrorMemoryAllocation)                                               \
-            return set_error(MSHQC_CD_ERR_ALLOC, "device allocation of " +                 \
-                                                     std::to_string((size_t)(nbytes)) +    \
-                                                     " bytes failed");                     \
-        if (_e != cudaSuccess) return cuda_error(_e, "workspace");                         \
-    } while (0)
-#define CD_RC(x)             \
-    do {                     \
-        int _rc = (x);       \
-        if (_rc) return _rc; \
-    } while (0)
 
 namespace {
 
@@ -426,6 +407,13 @@ int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
 }
 
 }  // namespace
+
+int invalidate_spin(mshqc_cd_ctx* ctx, int spin) {
+    ctx->spin[spin].invalidate();
+    ctx->diag_os_valid = false;
+    if (ctx->Y_spin == spin) ctx->Y_spin = -1;
+    return MSHQC_CD_OK;
+}
 
 int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
     CD_RC(require_inputs(ctx, spin));
