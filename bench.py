@@ -47,6 +47,9 @@ WORKLOADS = {
     "cdmp2_grad_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=True, precision="fp16x3"),
     # energy only (the CD-RMP2 drop-in), N=400, o=40, M=1600
     "cdrmp2_energy_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=False, precision="fp16x3"),
+    # differentiated CD-UMP2 (the OMP2 step): separate alpha / beta orbitals
+    "cdump2_grad_n600_o60_58_m2400": dict(N=600, o=60, ob=58, M=2400, gradient=True, precision="fp16x3",
+                                          kind="unrestricted"),
 }
 DEFAULT_WORKLOAD = "cdmp2_grad_n1000_o100_m4000"
 
@@ -72,6 +75,24 @@ def workload_flops(N, o, M, gradient):
     if not gradient:
         return flops_transform(N, o, M) + flops_energy(N, o, M)
     return 2 * flops_transform(N, o, M) + 2 * flops_energy(N, o, M) + flops_gamma(N, o, M)
+
+
+def unrestricted_parts(N, oa, ob, M):
+    """(transforms, integral tiles, Gamma) of the unrestricted energy +
+    gradient: both spins transformed forward and back; the backward forms
+    every same-spin and opposite-spin (ia|jb) once and Gamma_alpha, Gamma_beta
+    (two products for the opposite-spin block)."""
+    va, vb = N - oa, N - ob
+    tr = 2 * (flops_transform(N, oa, M) + flops_transform(N, ob, M))
+    tiles = 2.0 * M * (va * va * oa * oa + vb * vb * ob * ob + va * vb * oa * ob)
+    gam = 2.0 * M * (va * va * oa * oa + vb * vb * ob * ob + 2.0 * va * vb * oa * ob)
+    return tr, tiles, gam
+
+
+def workload_flops_w(w):
+    if w.get("kind") == "unrestricted":
+        return sum(unrestricted_parts(w["N"], w["o"], w["ob"], w["M"]))
+    return workload_flops(w["N"], w["o"], w["M"], w["gradient"])
 
 
 # ---------------------------------------------------------------------------
@@ -175,23 +196,30 @@ def run_reference_once(w, seed, nthreads):
     """One bounded sample of the workload on the reference's own CPU code:
     CholeskyOMP2's energy + orbital-gradient evaluation (t2, E, OPDM,
     generalized Fock, w_ai; src/mp2/cholesky_omp2.cc:441-466) for gradient
-    workloads, CholeskyRMP2::compute for energy workloads."""
+    workloads (separate alpha / beta orbitals for the unrestricted one),
+    CholeskyRMP2::compute for energy workloads."""
     from mshqc_b200 import synthetic as syn
     from oracle import ref
     N, o, M = REF_SAMPLE["N"], REF_SAMPLE["o"], REF_SAMPLE["M"]
+    unres = w.get("kind") == "unrestricted"
+    ob = o - 1 if unres else o
     base = syn.make_inputs(N, o, M, seed=seed)
     sig = syn.twin_sigma(N, o, M, base.alpha.eps)
-    inp = syn.make_inputs(N, o, M, seed=seed, sigma=sig)
+    inp = syn.make_inputs(N, o, M, seed=seed, sigma=sig, nocc_beta=ob if unres else None)
     a = inp.alpha
+    b = inp.beta if unres else a
     if w["gradient"]:
         H = np.eye(N)   # the cost of the Fock build does not depend on H
-        r = ref.omp2_pieces(inp.L, a.C, a.C, a.eps, a.eps, o, o, H, nthreads=nthreads)
+        r = ref.omp2_pieces(inp.L, a.C, b.C, a.eps, b.eps, o, ob, H, nthreads=nthreads)
         what = "CholeskyOMP2 energy + w_ai"
     else:
         r = ref.rmp2(inp.L, a.C, a.eps, o, nthreads=nthreads)
         what = "CholeskyRMP2::compute"
-    flops = workload_flops(N, o, M, w["gradient"])
-    return r["seconds"], flops, f"N={N}, o={o}, M={M} {what}"
+    if unres:
+        flops = sum(unrestricted_parts(N, o, ob, M))
+    else:
+        flops = workload_flops(N, o, M, w["gradient"])
+    return r["seconds"], flops, f"N={N}, o={o}{'/%d' % ob if unres else ''}, M={M} {what}"
 
 
 def bench_reference(args, w, rank, world):
@@ -238,13 +266,19 @@ def bench_gpu(args, w, rank, world, local_rank):
     N, o, M = w["N"], w["o"], w["M"]
     gradient = w["gradient"]
     prec = capi.PRECISIONS[w["precision"]]
+    unres = w.get("kind") == "unrestricted"
+    kind = capi.UNRESTRICTED if unres else capi.RESTRICTED
+    ob = w.get("ob", o)
     seed = 1000 + rank
 
     orb = syn.make_orbitals(N, o, seed)
+    orb_b = syn.make_orbitals(N, ob, seed + 7919) if unres else orb
     sigma = syn.twin_sigma(N, o, M, orb.eps)
     L_dev = syn.make_vectors_device(N, M, seed, sigma, dev)
     C_dev = torch.from_numpy(orb.C).to(dev)
     e_dev = torch.from_numpy(orb.eps).to(dev)
+    Cb_dev = torch.from_numpy(orb_b.C).to(dev)
+    eb_dev = torch.from_numpy(orb_b.eps).to(dev)
 
     stream = torch.cuda.Stream(device=dev)
     ctx = capi.Context(local_rank)
@@ -253,9 +287,11 @@ def bench_gpu(args, w, rank, world, local_rank):
 
     def step(context, precision, C, eps):
         context.set_orbitals(capi.ALPHA, C, eps, o)            # new orbitals: full recompute
+        if unres:
+            context.set_orbitals(capi.BETA, Cb_dev, eb_dev, ob)
         if gradient:
-            return context.mp2_gradient(capi.RESTRICTED, precision)
-        return context.mp2_energy(capi.RESTRICTED, precision)
+            return context.mp2_gradient(kind, precision)
+        return context.mp2_energy(kind, precision)
 
     def barrier():
         if world > 1:
@@ -293,7 +329,7 @@ def bench_gpu(args, w, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     elapsed = float(t.item())
-    flops = workload_flops(N, o, M, gradient)
+    flops = workload_flops_w(w)
     value = world * flops * args.steps / elapsed / 1e12
     mixed_res = r
 
@@ -311,13 +347,16 @@ def bench_gpu(args, w, rank, world, local_rank):
         ms64 = t0.elapsed_time(t1)
         if gradient:
             e3, e64 = mixed_res.energy["total"], r64.energy["total"]
+            pairs = [(mixed_res.dC_a, r64.dC_a, mixed_res.deps_a, r64.deps_a)]
+            if unres:
+                pairs.append((mixed_res.dC_b, r64.dC_b, mixed_res.deps_b, r64.deps_b))
             fp64 = {"fp64_ms_per_step": ms64, "fp64_tflops": flops / (ms64 / 1e3) / 1e12,
                     "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps),
                     "energy_fp64": e64, "energy_mixed": e3,
                     "energy_error_uEh": abs(e3 - e64) * 1e6,
-                    "max_abs_dC_error": float(np.max(np.abs(mixed_res.dC_a - r64.dC_a))),
-                    "max_abs_deps_error": float(np.max(np.abs(mixed_res.deps_a - r64.deps_a))),
-                    "max_abs_dC": float(np.max(np.abs(r64.dC_a)))}
+                    "max_abs_dC_error": max(float(np.max(np.abs(x - y))) for x, y, _, _ in pairs),
+                    "max_abs_deps_error": max(float(np.max(np.abs(x - y))) for _, _, x, y in pairs),
+                    "max_abs_dC": max(float(np.max(np.abs(y))) for _, y, _, _ in pairs)}
         else:
             fp64 = {"fp64_ms_per_step": ms64,
                     "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps),
@@ -330,6 +369,8 @@ def bench_gpu(args, w, rank, world, local_rank):
         L_host.copy_(L_dev)
         C_host = np.asfortranarray(orb.C)
         e_host = orb.eps.copy()
+        Cb_host = np.asfortranarray(orb_b.C)
+        eb_host = orb_b.eps.copy()
         del L_dev
         ctx.close()
         torch.cuda.empty_cache()
@@ -340,9 +381,11 @@ def bench_gpu(args, w, rank, world, local_rank):
         def step_e2e():
             ctx_h.set_vectors(L_np, nbf=N)
             ctx_h.set_orbitals(capi.ALPHA, C_host, e_host, o)
+            if unres:
+                ctx_h.set_orbitals(capi.BETA, Cb_host, eb_host, ob)
             if gradient:
-                return ctx_h.mp2_gradient(capi.RESTRICTED, prec)       # results copied to host
-            return ctx_h.mp2_energy(capi.RESTRICTED, prec)
+                return ctx_h.mp2_gradient(kind, prec)       # results copied to host
+            return ctx_h.mp2_energy(kind, prec)
 
         step_e2e()
         barrier()
@@ -356,8 +399,9 @@ def bench_gpu(args, w, rank, world, local_rank):
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
-        h2d = L_np.nbytes + C_host.nbytes + e_host.nbytes
-        d2h = 8 * 7 + ((N * N + N) * 8 if gradient else 0)
+        nspin = 2 if unres else 1
+        h2d = L_np.nbytes + nspin * (C_host.nbytes + e_host.nbytes)
+        d2h = 8 * 7 + (nspin * (N * N + N) * 8 if gradient else 0)
         e2e = {"value": world * flops * args.steps / e2e_elapsed / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": 1e3 * e2e_elapsed / args.steps}
@@ -368,8 +412,11 @@ def bench_gpu(args, w, rank, world, local_rank):
     # ---- roofline of the dominant kernel ----------------------------------
     peaks, peak_src = measured_peaks()
     st = {k: statistics.median(s[k] for s in stages) for k in stages[0]}
-    if gradient:
-        cand = {"amplitude": ("pair_energy_tc_kernel<AMPLITUDE>", 2.0 * (N - o) ** 2 * M * o * o),
+    if gradient and unres:
+        _, ftiles, fgam = unrestricted_parts(N, o, ob, M)
+        cand = {"amplitude": ("vtile_tc_kernel", ftiles), "gamma": ("gamma_tc_kernel", fgam)}
+    elif gradient:
+        cand = {"amplitude": ("vtile_tc_kernel", 2.0 * (N - o) ** 2 * M * o * o),
                 "gamma": ("gamma_tc_kernel", flops_gamma(N, o, M))}
     else:
         cand = {"pair_energy": ("pair_energy_tc_kernel<RESTRICTED>", flops_energy(N, o, M))}
@@ -394,7 +441,9 @@ def bench_gpu(args, w, rank, world, local_rank):
                       "fp16x3 (scaled fixed point, exact f32 accumulate; f64 denominators, sums)"),
             "data": "synthetic (seeded recipe, scaled twin, device Philox stream for L)",
             "config": {"workload": args.workload, "N": N, "o": o, "v": N - o, "M": M,
-                       "kind": "restricted", "precision": w["precision"], "gradient": gradient,
+                       **({"o_beta": ob} if unres else {}),
+                       "kind": "unrestricted" if unres else "restricted",
+                       "precision": w["precision"], "gradient": gradient,
                        "sigma": sigma, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (AO vectors %.1f GB, MO vectors %.2f GB)" % (
                            N * N * M * 8 / 1e9, o * (N - o) * M * 8 / 1e9),

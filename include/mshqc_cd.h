@@ -97,8 +97,9 @@ MSHQC_CD_API int mshqc_cd_device_bytes(mshqc_cd_ctx* ctx, int64_t* bytes);
 MSHQC_CD_API int mshqc_cd_launch_count(mshqc_cd_ctx* ctx, int64_t* count);
 /* Device time (ms, CUDA events) of the stages of the last energy or gradient
  * call: [0] half transforms, [1] fixed-point split, [2] pair-energy kernels,
- * [3] amplitude pass, [4] Gamma GEMM, [5] transposed transforms, [6] other.
- * n_out entries are written (at most 8). */
+ * [3] integral tiles of the backward, [4] Gamma GEMM, [5] transposed
+ * transforms, [6] other, [7] element-wise amplitude pass.  n_out entries are
+ * written (at most 8). */
 MSHQC_CD_API int mshqc_cd_stage_times(mshqc_cd_ctx* ctx, double* ms_out, int n_out);
 /* 1 when every tensor-core accumulation of the last mixed-precision call was
  * provably exact (Cauchy-Schwarz bound of the integer accumulators below

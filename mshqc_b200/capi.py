@@ -181,7 +181,8 @@ class Context:
         _check(self._lib.mshqc_cd_launch_count(self._h, ctypes.byref(c)))
         return int(c.value)
 
-    STAGES = ("transform", "split", "pair_energy", "amplitude", "gamma", "transposed", "other")
+    STAGES = ("transform", "split", "pair_energy", "amplitude", "gamma", "transposed", "other",
+              "amp_elem")
 
     def stage_times(self) -> dict:
         buf = (ctypes.c_double * 8)()
@@ -263,6 +264,24 @@ class Context:
             _ptr(dCb) if dCb is not None else None, _ptr(dea),
             _ptr(deb) if deb is not None else None, HOST))
         return Gradient(e.as_dict(), dCa, dCb, dea, deb)
+
+    def mp2_gradient_torch(self, kind: int = RESTRICTED, precision: int = FP64, device=None) -> Gradient:
+        """mp2_gradient with the derivatives written straight into CUDA
+        tensors on `device` (dC as an (N, N) tensor dC[mu, p])."""
+        import torch
+        N = self.nbf
+        e = Energy()
+        nspin = 2 if kind == UNRESTRICTED else 1
+        dCt = [torch.empty((N, N), dtype=torch.float64, device=device) for _ in range(nspin)]
+        de = [torch.empty(N, dtype=torch.float64, device=device) for _ in range(nspin)]
+        torch.cuda.current_stream(device).synchronize()
+        _check(self._lib.mshqc_cd_mp2_gradient(
+            self._h, kind, precision, ctypes.byref(e), _ptr(dCt[0]), _ptr(dCt[1]) if nspin == 2 else None,
+            _ptr(de[0]), _ptr(de[1]) if nspin == 2 else None, DEVICE))
+        # the library writes column-major dC: the tensor holds dC^T
+        dC = [t.t() for t in dCt]
+        return Gradient(e.as_dict(), dC[0], dC[1] if nspin == 2 else None, de[0],
+                        de[1] if nspin == 2 else None)
 
     # -- CD-OMP2 ------------------------------------------------------------
     def set_core_hamiltonian(self, H):

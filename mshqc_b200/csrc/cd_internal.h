@@ -158,7 +158,7 @@ struct mshqc_cd_ctx {
 };
 
 namespace mshqc_cd {
-enum Stage { ST_TRANSFORM = 0, ST_SPLIT, ST_PAIR, ST_AMPLITUDE, ST_GAMMA, ST_TRANSPOSED, ST_OTHER };
+enum Stage { ST_TRANSFORM = 0, ST_SPLIT, ST_PAIR, ST_AMPLITUDE, ST_GAMMA, ST_TRANSPOSED, ST_OTHER, ST_AMP_ELEM };
 // stage timing: begin_stage/end_stage record events on the context stream;
 // collect_stages (after a synchronize) folds them into ctx->stage_ms
 void reset_stages(mshqc_cd_ctx* ctx);

@@ -736,6 +736,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
         const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
         begin_stage(ctx, ST_AMPLITUDE);
         vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
+        end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
         AmpElemArgs e{};
@@ -754,6 +755,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
         }
         e.deps_x = deps_x;  e.deps_y = deps_y;
         e.partial = partial + (int64_t)i0 * tiles_per_i;
+        begin_stage(ctx, ST_AMP_ELEM);
         amp_elem_kernel<MODE, true><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
         end_stage(ctx);
         CD_CUDA(cudaGetLastError());
@@ -798,6 +800,7 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
         g.alpha = 1.0;  g.beta = 0.0;
         begin_stage(ctx, ST_AMPLITUDE);
         CD_CUDA(gemm_f64(g, true, true, ctx->stream));
+        end_stage(ctx);
         ctx->launches++;
         AmpElemArgs e{};
         e.S = ctx->W.as<double>();
@@ -810,6 +813,7 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
         e.A64 = ctx->amp.as<double>();  e.ldA = ldS;
         e.deps_x = deps_x;  e.deps_y = deps_y;
         e.partial = partial + (int64_t)i0 * tiles_per_i;
+        begin_stage(ctx, ST_AMP_ELEM);
         amp_elem_kernel<MODE, false><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
         end_stage(ctx);
         CD_CUDA(cudaGetLastError());
