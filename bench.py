@@ -5,21 +5,22 @@
     python bench.py --impl reference ...   # the reference CPU path
 
 Default workload: CD-MP2 energy plus the exact orbital gradient (dE/dC,
-dE/deps) of a closed-shell system with N=1000 basis functions, o=100
-occupied orbitals and M=4000 Cholesky vectors (the largest of the synthetic
-configurations whose FP64 AO vectors fit one GPU; the N=2000 one needs 256 GB
-of AO vectors), synthetic inputs of the seeded recipe in
-mshqc_b200/synthetic.py at the scaled magnitude |E_corr| ~ 0.05 o Eh.
+dE/deps) of a closed-shell system with N=2000 basis functions, o=200
+occupied orbitals and M=8000 Cholesky vectors, synthetic inputs of the seeded
+recipe (mshqc_b200/synthetic.py) at the scaled magnitude |E_corr| ~ 0.05 o Eh.
+Its FP64 AO vectors would take 256 GB, so the library generates them on the
+device chunk by chunk (mshqc_cd_gen_vectors) wherever they are read.
 
-One step = AO->MO half transform + fused amplitude/energy pass + Gamma GEMM +
-transposed transforms, i.e. one mp2_gradient call, in the mixed precision
-(scaled FP16x3 on the tensor cores).  The FP64 path is timed on the same
-inputs for the mixed-vs-FP64 comparison and the energy / gradient errors.
+One step = AO->MO half transform + integral tiles + amplitude pass + Gamma
+GEMM + transposed transforms, i.e. one mp2_gradient call, in the mixed
+precision (scaled FP16x3 on the tensor cores).  The FP64 path is timed once on
+the same inputs for the mixed-vs-FP64 comparison and the energy / gradient
+errors.
 
 `value` = FP64-equivalent algorithmic TFLOP/s over all ranks with the inputs
 resident in HBM (work 2 F_T + 2 F_E + 2 v^2 M o^2; F_T = 2 M N o (N+v),
-F_E = v^2 M o (o+1)); `e2e` = the same metric through the C ABI from pinned
-host buffers, copies inside the timed region.  Multi-GPU runs are replicas
+F_E = v^2 M o (o+1)); `e2e` = the same metric through the C ABI from host
+buffers, copies inside the timed region.  Multi-GPU runs are replicas
 (independent inputs per rank, weak scaling, no data-path collective).
 """
 from __future__ import annotations
@@ -41,7 +42,11 @@ sys.path.insert(0, ROOT)
 METRIC = "CD-MP2 energy+OMP2 grad s & TFLOP/s: mixed vs FP64 on B200 at ≤1 µEh"
 
 WORKLOADS = {
-    # headline: energy + exact gradient, mixed vs FP64
+    # the north-star size: energy + exact gradient, vectors generated on the
+    # device (their FP64 AO form, 256 GB, does not fit)
+    "cdmp2_grad_n2000_o200_m8000": dict(N=2000, o=200, M=8000, gradient=True, precision="fp16x3",
+                                        gen=True),
+    # energy + exact gradient, mixed vs FP64, stored vectors
     "cdmp2_grad_n1000_o100_m4000": dict(N=1000, o=100, M=4000, gradient=True, precision="fp16x3"),
     # smaller variant of the same step
     "cdmp2_grad_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=True, precision="fp16x3"),
@@ -51,7 +56,7 @@ WORKLOADS = {
     "cdump2_grad_n600_o60_58_m2400": dict(N=600, o=60, ob=58, M=2400, gradient=True, precision="fp16x3",
                                           kind="unrestricted"),
 }
-DEFAULT_WORKLOAD = "cdmp2_grad_n1000_o100_m4000"
+DEFAULT_WORKLOAD = "cdmp2_grad_n2000_o200_m8000"
 
 
 # ---------------------------------------------------------------------------
@@ -274,7 +279,8 @@ def bench_gpu(args, w, rank, world, local_rank):
     orb = syn.make_orbitals(N, o, seed)
     orb_b = syn.make_orbitals(N, ob, seed + 7919) if unres else orb
     sigma = syn.twin_sigma(N, o, M, orb.eps)
-    L_dev = syn.make_vectors_device(N, M, seed, sigma, dev)
+    gen = bool(w.get("gen"))
+    L_dev = None if gen else syn.make_vectors_device(N, M, seed, sigma, dev)
     C_dev = torch.from_numpy(orb.C).to(dev)
     e_dev = torch.from_numpy(orb.eps).to(dev)
     Cb_dev = torch.from_numpy(orb_b.C).to(dev)
@@ -283,7 +289,10 @@ def bench_gpu(args, w, rank, world, local_rank):
     stream = torch.cuda.Stream(device=dev)
     ctx = capi.Context(local_rank)
     ctx.set_stream(stream.cuda_stream)
-    ctx.set_vectors(L_dev)
+    if gen:
+        ctx.gen_vectors(N, M, seed, sigma)
+    else:
+        ctx.set_vectors(L_dev)
 
     def step(context, precision, C, eps):
         context.set_orbitals(capi.ALPHA, C, eps, o)            # new orbitals: full recompute
@@ -336,7 +345,8 @@ def bench_gpu(args, w, rank, world, local_rank):
     # ---- FP64 path on the same inputs (comparison and error) ---------------
     fp64 = {}
     if prec != capi.FP64 and not args.no_fp64:
-        step(ctx, capi.FP64, C_dev, e_dev)                       # warm
+        # one FP64 step, not warmed up: the same transforms ran above and the
+        # FP64 kernels' first-launch cost is negligible next to the step
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
@@ -365,8 +375,9 @@ def bench_gpu(args, w, rank, world, local_rank):
     # ---- end to end through the C ABI from pinned host buffers ------------
     e2e = None
     if not args.no_e2e:
-        L_host = torch.empty(L_dev.shape, dtype=torch.float64, pin_memory=True)
-        L_host.copy_(L_dev)
+        if not gen:
+            L_host = torch.empty(L_dev.shape, dtype=torch.float64, pin_memory=True)
+            L_host.copy_(L_dev)
         C_host = np.asfortranarray(orb.C)
         e_host = orb.eps.copy()
         Cb_host = np.asfortranarray(orb_b.C)
@@ -376,10 +387,13 @@ def bench_gpu(args, w, rank, world, local_rank):
         torch.cuda.empty_cache()
         ctx_h = capi.Context(local_rank)
         ctx_h.set_stream(stream.cuda_stream)
-        L_np = L_host.numpy()
+        L_np = None if gen else L_host.numpy()
 
         def step_e2e():
-            ctx_h.set_vectors(L_np, nbf=N)
+            if gen:
+                ctx_h.gen_vectors(N, M, seed, sigma)
+            else:
+                ctx_h.set_vectors(L_np, nbf=N)
             ctx_h.set_orbitals(capi.ALPHA, C_host, e_host, o)
             if unres:
                 ctx_h.set_orbitals(capi.BETA, Cb_host, eb_host, ob)
@@ -400,7 +414,7 @@ def bench_gpu(args, w, rank, world, local_rank):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
         nspin = 2 if unres else 1
-        h2d = L_np.nbytes + nspin * (C_host.nbytes + e_host.nbytes)
+        h2d = (0 if gen else L_np.nbytes) + nspin * (C_host.nbytes + e_host.nbytes)
         d2h = 8 * 7 + (nspin * (N * N + N) * 8 if gradient else 0)
         e2e = {"value": world * flops * args.steps / e2e_elapsed / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -445,8 +459,10 @@ def bench_gpu(args, w, rank, world, local_rank):
                        "kind": "unrestricted" if unres else "restricted",
                        "precision": w["precision"], "gradient": gradient,
                        "sigma": sigma, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (AO vectors %.1f GB, MO vectors %.2f GB)" % (
-                           N * N * M * 8 / 1e9, o * (N - o) * M * 8 / 1e9),
+                       "vectors": "generated on the device per chunk" if gen else "stored",
+                       "l2": "inputs larger than L2 (AO vectors %.1f GB%s, MO vectors %.2f GB)" % (
+                           N * N * M * 8 / 1e9, ", regenerated, never stored" if gen else "",
+                           o * (N - o) * M * 8 / 1e9),
                        "stage_ms": st, "mixed_exact_accumulation": exact, **fp64},
             "clocks": clk,
             "e2e": e2e,

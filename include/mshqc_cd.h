@@ -112,6 +112,27 @@ MSHQC_CD_API int mshqc_cd_mixed_exact(mshqc_cd_ctx* ctx, int* exact);
  * src/mp2/cholesky_ump2.cc:250, src/mp2/cholesky_omp2.cc:77). */
 MSHQC_CD_API int mshqc_cd_set_vectors(mshqc_cd_ctx* ctx, const double* L, int64_t nbf,
                          int64_t nvec, int layout, int where);
+/* Pivoted incomplete Cholesky decomposition of the ERI matrix, FP64 on the
+ * device: CholeskyERI::decompose (reference src/integrals/cholesky_eri.cc:40-149;
+ * first-index pivot :155-167, new vector :169-203, clamped diagonal update
+ * :108-109).  eri: N^4 doubles, element (ij|kl) at ((i N + j) N + k) N + l.
+ * Stops when the largest remaining diagonal is below threshold (or after N^2
+ * vectors; *converged tells which).  The vectors become the context's
+ * vectors (as after mshqc_cd_set_vectors) and, when L_out is not NULL, are
+ * copied there (max_vectors * N^2 doubles of room, vector Q at Q N^2). */
+MSHQC_CD_API int mshqc_cd_cholesky_decompose(mshqc_cd_ctx* ctx, const double* eri, int64_t nbf,
+                                             double threshold, double* L_out, int64_t max_vectors,
+                                             int64_t* n_vectors, int* converged, int where);
+/* Synthetic Cholesky vectors generated on the device instead of uploaded
+ * (no counterpart in the reference, which takes them as data): L^Q = sigma
+ * 10^(-6 Q / nvec) (X^Q + X^Q^T)/2, X^Q_{mu nu} standard normal from the
+ * counter-based Philox4x32-10 generator (key = seed, counter =
+ * (Q nbf + mu) nbf + nu) and Box-Muller.  The vectors are never stored: the
+ * consumers regenerate the chunks they read, so sizes whose FP64 vectors
+ * exceed device memory run (nbf = 2000, nvec = 8000: 256 GB).  The OMP2
+ * entry points need stored vectors. */
+MSHQC_CD_API int mshqc_cd_gen_vectors(mshqc_cd_ctx* ctx, int64_t nbf, int64_t nvec, uint64_t seed,
+                                      double sigma);
 /* Orbitals of one spin.  Replaces the SCFResult fields C_alpha/C_beta,
  * orbital_energies_alpha/beta, n_occ_alpha/beta read by the MP2 classes
  * (reference src/mp2/cholesky_rmp2.cc:27-29,77-78,106;

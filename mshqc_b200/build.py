@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmshqc_cuda.so")
 
-CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_omp2.cu", "cd_noalloc.cu"]
+CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_omp2.cu", "cd_vectors.cu", "cd_decompose.cu", "cd_noalloc.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -78,11 +78,40 @@ def build_cuda(verbose: bool = False, force: bool = False, extra_flags=()) -> st
     return LIB
 
 
+CPP_DIR = os.path.join(HERE, "cpp")
+CPP_SOURCES = ["mshqc_b200.cc", "bindings.cc"]
+
+
+def module_path() -> str:
+    return os.path.join(HERE, "_mshqc" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_module(verbose: bool = False, force: bool = False) -> str:
+    """The pybind11 module mshqc_b200._mshqc (the C++ mirror classes), linked
+    against libmshqc_cuda.so next to it (rpath $ORIGIN/lib)."""
+    import pybind11
+    target = module_path()
+    deps = [os.path.join(CPP_DIR, f) for f in os.listdir(CPP_DIR)] + [LIB,
+                                                                      os.path.join(ROOT, "include", "mshqc_cd.h")]
+    if not force and not _stale(target, deps):
+        return target
+    gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+    cmd = [gxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+           *[os.path.join(CPP_DIR, f) for f in CPP_SOURCES],
+           "-L", LIBDIR, "-lmshqc_cuda", "-Wl,-rpath,$ORIGIN/lib", "-o", target + ".tmp"]
+    _run(cmd, verbose)
+    os.replace(target + ".tmp", target)
+    return target
+
+
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
     force = "--force" in argv
     lib = build_cuda(verbose=True, force=force)
     print("built", lib)
+    mod = build_module(verbose=True, force=force)
+    print("built", mod)
 
 
 if __name__ == "__main__":

@@ -76,6 +76,9 @@ SIGNATURES = {
     "mshqc_cd_pair_energies": (_i32, [_vp, _i32, _vp, _i32]),
     "mshqc_cd_mp2_gradient": (_i32, [_vp, _i32, _i32, ctypes.POINTER(Energy), _vp, _vp, _vp,
                                      _vp, _i32]),
+    "mshqc_cd_gen_vectors": (_i32, [_vp, _i64, _i64, ctypes.c_uint64, ctypes.c_double]),
+    "mshqc_cd_cholesky_decompose": (_i32, [_vp, _vp, _i64, ctypes.c_double, _vp, _i64,
+                                           ctypes.POINTER(_i64), ctypes.POINTER(_i32), _i32]),
     "mshqc_cd_set_core_hamiltonian": (_i32, [_vp, _vp, _i32]),
     "mshqc_cd_get_orbitals": (_i32, [_vp, _i32, _vp, _i32]),
     "mshqc_cd_omp2_pieces": (_i32, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double), _vp, _vp, _vp, _vp,
@@ -211,6 +214,27 @@ class Context:
             nbf = int(round(per ** 0.5)) if lay == LAYOUT_FULL else int((np.sqrt(8 * per + 1) - 1) / 2)
         _check(self._lib.mshqc_cd_set_vectors(self._h, _ptr(L), int(nbf), int(M), lay, where))
         self.nbf, self.nvec = int(nbf), int(M)
+        return self
+
+    def cholesky_decompose(self, eri, threshold: float = 1e-6):
+        """Pivoted Cholesky of eri[i, j, k, l] = (ij|kl) on the device; the
+        vectors (M, N*N) are returned and become the context's vectors."""
+        E = _host_f64(eri)
+        N = E.shape[0]
+        out = np.empty((N * N, N * N), dtype=np.float64)
+        m = ctypes.c_int64(0)
+        conv = ctypes.c_int(0)
+        _check(self._lib.mshqc_cd_cholesky_decompose(self._h, _ptr(E), N, float(threshold), _ptr(out), N * N,
+                                                      ctypes.byref(m), ctypes.byref(conv), HOST))
+        self.nbf, self.nvec = N, int(m.value)
+        self.decompose_converged = bool(conv.value)
+        return out[:m.value].copy()
+
+    def gen_vectors(self, nbf: int, nvec: int, seed: int, sigma: float = 1.0):
+        """Synthetic vectors generated on the device (never stored); the
+        numpy twin is synthetic.make_vectors_philox."""
+        _check(self._lib.mshqc_cd_gen_vectors(self._h, int(nbf), int(nvec), int(seed), float(sigma)))
+        self.nbf, self.nvec = int(nbf), int(nvec)
         return self
 
     def set_orbitals(self, spin: int, C, eps, nocc: int):

@@ -2,9 +2,8 @@
 //
 // Input: a staging block of integrals S[(i - i0, a)][(j, b)] = (ia|jb) for
 // the occupied rows i of one block and every j (FP32 from vtile_tc.cuh, or
-// FP64 from the FP64 GEMM).  One CTA of 256 threads takes one 32 x 32 tile of
-// (a, b) of one pair (i, j); with D = e_i + e_j - e_a - e_b (|D| < 1e-12
-// skipped, reference src/mp2/cholesky_rmp2.cc:139):
+// FP64 from the FP64 GEMM), 32 x 32 tiles with D = e_i + e_j - e_a - e_b
+// (|D| < 1e-12 skipped, reference src/mp2/cholesky_rmp2.cc:139):
 //
 //   RESTRICTED     V = (ia|jb), W = (ib|ja); t = V/D, amplitude tt = (2V - W)/D,
 //                  energy V tt, r = t tt          (dE/dB = 4 Gamma)
@@ -20,8 +19,11 @@
 // K-major layout of the tensor-core Gamma kernel (SPLIT), or FP64 row-major
 // [(i - i0, a)][(j, b)] for the FP64 GEMM.  OPPOSITE_SPIN with SPLIT also
 // writes the transposed operand [(j, b)][(i - i0, a)] for Gamma_beta.
-// dE/de gets -r on i and j and +r on a and b (atomics); the tile's energy goes
-// to partial[tile] and a deterministic reduction adds the tiles up.
+// One CTA of 256 threads takes one pair (i, j) and walks its 32 x 32 tiles of
+// (a, b), column block outer; the pair's energy, its row sums
+// sum_b r (per a), column sums sum_a r (per b) and total sum r go to per-pair
+// buffers, each written by one thread, and deps_*_kernel turn them into
+// dE/de (+r on a and b, -r on i and j) in a fixed order.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -46,8 +48,10 @@ struct AmpElemArgs {
     uint16_t* Ahi; uint16_t* Alo; long long RA;   // SPLIT: rows R = ii*rsx + a, K = j*ksy + b
     uint16_t* Thi; uint16_t* Tlo; long long RT;   // SPLIT, OPPOSITE_SPIN: rows j*ksy + b, K = ii*rsx + a
     double* A64; long long ldA;                   // FP64: [R][K]
-    double* deps_x; double* deps_y;               // occupied then virtual (same array when X = Y)
-    double* partial;        // [nbi * oy * (rsx/32) * (ksy/32)]
+    double* partial;        // [ox * oy] energy of each pair (i, j), i over all row orbitals
+    double* prow;           // [ox * oy][rsx] sum_b r per pair and row a (or null)
+    double* pcol;           // [ox * oy][ksy] sum_a r per pair and column b (or null)
+    double* pocc;           // [ox * oy] sum_ab r per pair (or null)
 };
 
 namespace amp_detail {
@@ -79,85 +83,101 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
     __shared__ TS Vt[32][33];
     __shared__ TS Wt[MODE == AMP_OPPOSITE_SPIN ? 1 : 32][33];
     __shared__ double T[32][33];
-    __shared__ double rsum_s[32], csum_s[32], red_e[8], red_r[8];
+    __shared__ double colpart[8][33];
+    __shared__ double red_e[8], red_r[8];
     const TS* S = static_cast<const TS*>(p.S);
     const int ta = p.rsx / 32, tb = p.ksy / 32;
-    const long long tile = blockIdx.x;
-    const long long pr = tile / ((long long)ta * tb);
-    const int tab = (int)(tile % ((long long)ta * tb));
-    const int ii = (int)(pr / p.oy), j = (int)(pr % p.oy), i = p.i0 + ii;
-    const int a0 = (tab / tb) * 32, b0 = (tab % tb) * 32;
+    const int ii = (int)(blockIdx.x / p.oy), j = (int)(blockIdx.x % p.oy), i = p.i0 + ii;
+    const long long pair = (long long)i * p.oy + j;          // over all occupied rows
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
-    if (threadIdx.x < 32) {
-        rsum_s[threadIdx.x] = 0.0;
-        csum_s[threadIdx.x] = 0.0;
-    }
-#pragma unroll
-    for (int r = ty; r < 32; r += 8) {
-        Vt[r][tx] = S[((long long)ii * p.rsx + a0 + r) * p.ldS + (long long)j * p.csy + b0 + tx];
-        if (MODE != AMP_OPPOSITE_SPIN)   // (ib|ja): rows (i, b), columns (j, a)
-            Wt[r][tx] = S[((long long)ii * p.rsx + b0 + r) * p.ldS + (long long)j * p.csy + a0 + tx];
-    }
-    __syncthreads();
     const double eij = p.eox[i] + p.eoy[j];
+    double* prow = p.prow ? p.prow + pair * p.rsx : nullptr;
+    double* pcol = p.pcol ? p.pcol + pair * p.ksy : nullptr;
     double esum = 0.0, rtot = 0.0;
+    for (int yb = 0; yb < tb; ++yb) {
+        const int b0 = yb * 32;
+        double cpart = 0.0;   // column b0 + tx over this thread's rows of every row block
+        for (int xb = 0; xb < ta; ++xb) {
+            const int a0 = xb * 32;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int r = ty * 4 + k;
-        const int a = a0 + r, b = b0 + tx;
-        double amp = 0.0, rr = 0.0;
-        if (a < p.vx && b < p.vy) {
-            const double D = eij - p.evx[a] - p.evy[b];
-            if (fabs(D) >= kDenomSkip) {
-                const double V = (double)Vt[r][tx];
-                const double rD = 1.0 / D;
-                if (MODE == AMP_RESTRICTED) {
-                    const double W = (double)Wt[tx][r];
-                    const double t = V * rD;
-                    amp = (2.0 * V - W) * rD;
-                    rr = t * amp;
-                    esum = fma(V, amp, esum);
-                } else if (MODE == AMP_SAME_SPIN) {
-                    const double W = (double)Wt[tx][r];
-                    const double g = V - W;
-                    amp = g * rD;
-                    rr = 0.25 * amp * amp;
-                    esum = fma(0.25 * g, amp, esum);
-                } else {
-                    amp = V * rD;
-                    rr = amp * amp;
-                    esum = fma(V, amp, esum);
+            for (int r = ty; r < 32; r += 8) {
+                Vt[r][tx] = S[((long long)ii * p.rsx + a0 + r) * p.ldS + (long long)j * p.csy + b0 + tx];
+                if (MODE != AMP_OPPOSITE_SPIN)   // (ib|ja): rows (i, b), columns (j, a)
+                    Wt[r][tx] = S[((long long)ii * p.rsx + b0 + r) * p.ldS + (long long)j * p.csy + a0 + tx];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int r = ty * 4 + k;
+                const int a = a0 + r, b = b0 + tx;
+                double amp = 0.0, rr = 0.0;
+                if (a < p.vx && b < p.vy) {
+                    const double D = eij - p.evx[a] - p.evy[b];
+                    if (fabs(D) >= kDenomSkip) {
+                        const double V = (double)Vt[r][tx];
+                        const double rD = 1.0 / D;
+                        if (MODE == AMP_RESTRICTED) {
+                            const double W = (double)Wt[tx][r];
+                            const double t = V * rD;
+                            amp = (2.0 * V - W) * rD;
+                            rr = t * amp;
+                            esum = fma(V, amp, esum);
+                        } else if (MODE == AMP_SAME_SPIN) {
+                            const double W = (double)Wt[tx][r];
+                            const double g = V - W;
+                            amp = g * rD;
+                            rr = 0.25 * amp * amp;
+                            esum = fma(0.25 * g, amp, esum);
+                        } else {
+                            amp = V * rD;
+                            rr = amp * amp;
+                            esum = fma(V, amp, esum);
+                        }
+                    }
+                }
+                T[r][tx] = amp;
+                rtot += rr;
+                cpart += rr;
+                double rs = rr;
+#pragma unroll
+                for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
+                // row a is always summed by lane 0 of warp ty: single writer, program order
+                if (prow && tx == 0) prow[a] = (yb == 0 ? 0.0 : prow[a]) + rs;
+                if (!SPLIT) p.A64[((long long)ii * p.rsx + a) * p.ldA + (long long)j * p.ksy + b] = amp;
+            }
+            if (SPLIT) {
+                __syncthreads();
+                // 32 rows x 4 groups of 8 K = 128 core-matrix rows per operand
+                if (threadIdx.x < 128) {
+                    const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
+                    const long long R = (long long)ii * p.rsx + a0 + r;
+                    const long long kc = (long long)j * p.ksy + b0 + g * 8;
+                    const long long off = amp_detail::blocked_offset(R, kc, p.RA);
+                    amp_detail::store_hilo8(&T[r][g * 8], p.Ahi + off, p.Alo + off);
+                } else if (MODE == AMP_OPPOSITE_SPIN) {
+                    const int w = threadIdx.x - 128;
+                    const int r = w >> 2, g = w & 3;   // r: b offset, g: group of 8 a
+                    const long long R = (long long)j * p.ksy + b0 + r;
+                    const long long kc = (long long)ii * p.rsx + a0 + g * 8;
+                    const long long off = amp_detail::blocked_offset(R, kc, p.RT);
+                    double col[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) col[e] = T[g * 8 + e][r];
+                    amp_detail::store_hilo8(col, p.Thi + off, p.Tlo + off);
                 }
             }
+            __syncthreads();   // Vt, Wt, T are refilled by the next tile
         }
-        T[r][tx] = amp;
-        rtot += rr;
-        double rs = rr;
+        if (pcol) {
+            colpart[ty][tx] = cpart;
+            __syncthreads();
+            if (ty == 0) {
+                double c = 0.0;
 #pragma unroll
-        for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
-        if (tx == 0) rsum_s[r] = rs;
-        if (rr != 0.0) atomicAdd(&csum_s[tx], rr);
-        if (!SPLIT) p.A64[((long long)ii * p.rsx + a) * p.ldA + (long long)j * p.ksy + b] = amp;
-    }
-    __syncthreads();
-    if (SPLIT) {
-        // 32 rows x 4 groups of 8 K = 128 core-matrix rows per operand
-        if (threadIdx.x < 128) {
-            const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
-            const long long R = (long long)ii * p.rsx + a0 + r;
-            const long long kc = (long long)j * p.ksy + b0 + g * 8;
-            const long long off = amp_detail::blocked_offset(R, kc, p.RA);
-            amp_detail::store_hilo8(&T[r][g * 8], p.Ahi + off, p.Alo + off);
-        } else if (MODE == AMP_OPPOSITE_SPIN) {
-            const int w = threadIdx.x - 128;
-            const int r = w >> 2, g = w & 3;   // r: b offset, g: group of 8 a
-            const long long R = (long long)j * p.ksy + b0 + r;
-            const long long kc = (long long)ii * p.rsx + a0 + g * 8;
-            const long long off = amp_detail::blocked_offset(R, kc, p.RT);
-            double col[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) col[e] = T[g * 8 + e][r];
-            amp_detail::store_hilo8(col, p.Thi + off, p.Tlo + off);
+                for (int w = 0; w < 8; ++w) c += colpart[w][tx];
+                pcol[b0 + tx] = c;
+            }
+            __syncthreads();
         }
     }
 #pragma unroll
@@ -170,22 +190,42 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
         red_r[ty] = rtot;
     }
     __syncthreads();
-    if (threadIdx.x < 32) {
-        const int a = a0 + threadIdx.x, b = b0 + threadIdx.x;
-        if (a < p.vx && rsum_s[threadIdx.x] != 0.0) atomicAdd(&p.deps_x[p.ox + a], rsum_s[threadIdx.x]);
-        if (b < p.vy && csum_s[threadIdx.x] != 0.0) atomicAdd(&p.deps_y[p.oy + b], csum_s[threadIdx.x]);
-    }
     if (threadIdx.x == 0) {
         double e = 0.0, r = 0.0;
         for (int w = 0; w < 8; ++w) {
             e += red_e[w];
             r += red_r[w];
         }
-        p.partial[tile] = e;
-        if (r != 0.0) {
-            atomicAdd(&p.deps_x[i], -r);
-            atomicAdd(&p.deps_y[j], -r);
-        }
+        p.partial[pair] = e;
+        if (p.pocc) p.pocc[pair] = r;
+    }
+}
+
+// dE/de from the per-pair sums, in a fixed order (no atomics):
+// deps_x[ox + a] += sum_pairs prow, deps_y[oy + b] += sum_pairs pcol,
+// deps_x[i] -= sum_j pocc[i][j], deps_y[j] -= sum_i pocc[i][j]
+static __global__ void deps_rows_kernel(const double* __restrict__ prow, long long npairs, int rsx, int v,
+                                        double* __restrict__ dvir) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= v) return;
+    double s = 0.0;
+    for (long long q = 0; q < npairs; ++q) s += prow[q * rsx + a];
+    dvir[a] += s;
+}
+
+// (dx and dy may be the same array: thread t touches only element t of each)
+static __global__ void deps_occ_kernel(const double* __restrict__ pocc, int ox, int oy, double* __restrict__ dx,
+                                       double* __restrict__ dy) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ox) {
+        double s = 0.0;
+        for (int j = 0; j < oy; ++j) s += pocc[(long long)t * oy + j];
+        dx[t] -= s;
+    }
+    if (t < oy) {
+        double s = 0.0;
+        for (int i = 0; i < ox; ++i) s += pocc[(long long)i * oy + t];
+        dy[t] -= s;
     }
 }
 

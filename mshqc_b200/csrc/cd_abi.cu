@@ -380,6 +380,7 @@ int mshqc_cd_set_vectors(mshqc_cd_ctx* ctx, const double* L, int64_t nbf, int64_
     ctx->M = M;
     ctx->Mp = round_up(M, 16);
     ctx->L_set = true;
+    ctx->L_gen = false;
     CD_CUDA(cudaStreamSynchronize(ctx->stream));
     return MSHQC_CD_OK;
 }

@@ -69,7 +69,11 @@ struct mshqc_cd_ctx {
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, int>> ev_marks;   // (stage, index of the start event)
     size_t ev_used = 0;
-    mshqc_cd::DevBuf L;             // [Q][N*N] FP64
+    mshqc_cd::DevBuf L;             // [Q][N*N] FP64 (stored vectors)
+    bool L_gen = false;             // vectors generated on the device, never stored
+    uint64_t gen_seed = 0;
+    mshqc_cd::DevBuf gen_scale;     // sigma * 10^(-6 Q / M) per Q (generated vectors)
+    mshqc_cd::DevBuf Lchunk;        // one generated chunk of vectors
     mshqc_cd::SpinState spin[2];
 
     // workspaces
@@ -87,6 +91,7 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf BT_b;          // backward: the same for beta
     mshqc_cd::DevBuf amp2;          // backward: second half of the staging (lo)
     mshqc_cd::DevBuf ampT, ampT2;   // backward: transposed opposite-spin amplitudes (hi, lo)
+    mshqc_cd::DevBuf dsum;          // backward: per-pair row / column / total sums for dE/de
     mshqc_cd::DevBuf W;             // backward: integral staging / C_vir-contracted Gamma
     mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
     mshqc_cd::DevBuf diag_os;       // sum_Q B_alpha[i][a] B_beta[i][a] (opposite-spin diagonal)
@@ -136,6 +141,7 @@ struct mshqc_cd_ctx {
         BT_b.release();
         ampT.release();
         ampT2.release();
+        dsum.release();
         W.release();
         for (auto& s : spin) {
             s.C.release();
@@ -149,6 +155,8 @@ struct mshqc_cd_ctx {
         }
         diag_os.release();
         Hcore.release();
+        gen_scale.release();
+        Lchunk.release();
         opdm.release();
         omp2_ws.release();
         Zt.release();
@@ -199,4 +207,10 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
 int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out,
                  double* dC_a, double* dC_b, double* deps_a, double* deps_b, int where);
 int invalidate_spin(mshqc_cd_ctx* ctx, int spin);   // orbitals of `spin` changed on the device
+
+// implemented in cd_vectors.cu: the vectors Q0 .. Q0 + mc - 1 (N*N doubles
+// each, contiguous): the stored array, or a chunk generated into ctx->Lchunk
+// (valid until the next call); vectors_chunk_size is the chunk to ask for.
+int64_t vectors_chunk_size(const mshqc_cd_ctx* ctx);
+int vectors_chunk(mshqc_cd_ctx* ctx, int64_t Q0, int64_t mc, const double** out);
 }  // namespace mshqc_cd

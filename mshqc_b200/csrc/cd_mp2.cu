@@ -51,18 +51,24 @@ int transform_f64(mshqc_cd_ctx* ctx, int spin) {
     CD_ALLOC(s.B64, sizeof(double) * (size_t)o * vp * Mp, true);
     s.vp = vp;
     const double* C = s.C.as<double>();
-    // Y[i][(Q,nu)] = sum_mu C[mu,i] L[Q][nu*N + mu]
-    GemmF64Args g1{};
-    g1.M = (int)o;
-    g1.N = (int)(M * N);
-    g1.K = (int)N;
-    g1.batch = 1;
-    g1.A = C;  g1.lda = N;  g1.sA = 0;
-    g1.B = ctx->L.as<double>();  g1.ldb = N;  g1.sB = 0;
-    g1.C = ctx->Y.as<double>();  g1.ldc = M * N;  g1.sC = 0;
-    g1.alpha = 1.0;  g1.beta = 0.0;
-    CD_CUDA(gemm_f64(g1, true, true, ctx->stream));
-    ctx->launches++;
+    // Y[i][(Q,nu)] = sum_mu C[mu,i] L[Q][nu*N + mu], one chunk of Q at a time
+    const int64_t qc = vectors_chunk_size(ctx);
+    for (int64_t Q0 = 0; Q0 < M; Q0 += qc) {
+        const int64_t mc = std::min(qc, M - Q0);
+        const double* Lc = nullptr;
+        CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
+        GemmF64Args g1{};
+        g1.M = (int)o;
+        g1.N = (int)(mc * N);
+        g1.K = (int)N;
+        g1.batch = 1;
+        g1.A = C;  g1.lda = N;  g1.sA = 0;
+        g1.B = Lc;  g1.ldb = N;  g1.sB = 0;
+        g1.C = ctx->Y.as<double>() + Q0 * N;  g1.ldc = M * N;  g1.sC = 0;
+        g1.alpha = 1.0;  g1.beta = 0.0;
+        CD_CUDA(gemm_f64(g1, true, true, ctx->stream));
+        ctx->launches++;
+    }
     // B[i][a][Q] = sum_nu C[nu, o+a] Y[i][Q][nu]
     GemmF64Args g2{};
     g2.M = (int)v;
@@ -302,15 +308,6 @@ UnitTables make_tables_tc(int mode, int ox, int oy, int nbx, int nby) {
     return t;
 }
 
-UnitTables make_tables_amp(int i0, int nbi, int o, int nb) {
-    UnitTables t;
-    for (int i = i0; i < i0 + nbi; ++i)
-        for (int j = 0; j < o; ++j) t.pairs.push_back(make_int2(i, j));
-    for (int x = 0; x < nb; ++x)
-        for (int y = 0; y < nb; ++y) t.blocks.push_back(make_int2(x, y));
-    return t;
-}
-
 template <int MODE>
 cudaError_t launch_tc(const PairTcArgs& a, int grid, cudaStream_t st) {
     const size_t smem = pair_tc::SMEM_BYTES;
@@ -521,9 +518,28 @@ int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC)
         ctx->launches++;
         ctx->Y_spin = -1;
     }
-    // dC[mu, i] = scale sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]: only o rows, so the
-    // long K = M*N is split over S independent partial products (batched
-    // GEMM) that a deterministic reduction adds up
+    // dC[mu, i] = scale sum_{(Q,nu)} W[i][(Q,nu)] L[(Q,nu)][mu]
+    if (ctx->L_gen) {
+        // generated vectors: one GEMM per chunk of Q, accumulated in order
+        const int64_t qc = vectors_chunk_size(ctx);
+        for (int64_t Q0 = 0; Q0 < M; Q0 += qc) {
+            const int64_t mc = std::min(qc, M - Q0);
+            const double* Lc = nullptr;
+            CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
+            GemmF64Args g{};
+            g.M = (int)o;  g.N = (int)N;  g.K = (int)(mc * N);  g.batch = 1;
+            g.A = ctx->Y.as<double>() + Q0 * N;  g.lda = M * N;  g.sA = 0;
+            g.B = Lc;  g.ldb = N;  g.sB = 0;
+            g.C = dC;  g.ldc = N;  g.sC = 0;
+            g.alpha = scale;  g.beta = Q0 == 0 ? 0.0 : 1.0;
+            CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+            ctx->launches++;
+        }
+        return MSHQC_CD_OK;
+    }
+    // stored vectors: only o rows, so the long K = M*N is split over S
+    // independent partial products (batched GEMM) that a deterministic
+    // reduction adds up
     {
         const int64_t K = M * N;
         const int64_t tiles = cdiv(o, 64) * cdiv(N, 64);
@@ -560,7 +576,7 @@ int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC)
 // deps (N, device) are written; *energy gets the closed-shell E.
 int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
     SpinState& s = ctx->spin[0];
-    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
+    const int64_t N = ctx->N, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
     const int nb = (int)(vp / 64);
     // occupied block size for the amplitude staging buffer
     size_t free_b = 0, total_b = 0;
@@ -686,6 +702,21 @@ int launch_gamma(mshqc_cd_ctx* ctx, const uint16_t* ahi, const uint16_t* alo, in
     return MSHQC_CD_OK;
 }
 
+// dE/de of one backward pass from its per-pair sums (amp_elem.cuh)
+int reduce_deps(mshqc_cd_ctx* ctx, const double* prow, const double* pcol, const double* pocc, int64_t ox,
+                int64_t oy, int64_t rsx, int64_t ksy, int64_t vx, int64_t vy, double* deps_x, double* deps_y) {
+    const int64_t npairs = ox * oy;
+    deps_rows_kernel<<<(unsigned)cdiv(vx, 128), 128, 0, ctx->stream>>>(prow, npairs, (int)rsx, (int)vx,
+                                                                       deps_x + ox);
+    deps_rows_kernel<<<(unsigned)cdiv(vy, 128), 128, 0, ctx->stream>>>(pcol, npairs, (int)ksy, (int)vy,
+                                                                       deps_y + oy);
+    deps_occ_kernel<<<(unsigned)cdiv(std::max(ox, oy), 128), 128, 0, ctx->stream>>>(pocc, (int)ox, (int)oy,
+                                                                                    deps_x, deps_y);
+    CD_CUDA(cudaGetLastError());
+    ctx->launches += 3;
+    return MSHQC_CD_OK;
+}
+
 // One mixed-precision backward pass: the occupied rows i of spin sx in
 // blocks against every j of spin sy.  Per block: (ia|jb) tiles on the tensor
 // cores (exact fixed point, FP32 staging), the element-wise amplitude pass,
@@ -715,7 +746,11 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
         CD_ALLOC(ctx->ampT, per_i_t * bi, false);
         CD_ALLOC(ctx->ampT2, per_i_t * bi, false);
     }
-    const int64_t tiles_per_i = dy.o * (dx.VR / 32) * (dy.VR / 32);
+    const int64_t npairs = dx.o * dy.o;
+    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.VR + dy.VR + 1)), false);
+    double* prow = ctx->dsum.as<double>();
+    double* pcol = prow + npairs * dx.VR;
+    double* pocc = pcol + npairs * dy.VR;
     const size_t vsm = vtile_tc::SMEM_BYTES;
     CD_CUDA(cudaFuncSetAttribute(vtile_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
     for (int i0 = 0; i0 < dx.o; i0 += bi) {
@@ -753,10 +788,10 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             e.Thi = ctx->ampT.as<uint16_t>();  e.Tlo = ctx->ampT2.as<uint16_t>();
             e.RT = (long long)KA;
         }
-        e.deps_x = deps_x;  e.deps_y = deps_y;
-        e.partial = partial + (int64_t)i0 * tiles_per_i;
+        e.partial = partial;
+        e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
         begin_stage(ctx, ST_AMP_ELEM);
-        amp_elem_kernel<MODE, true><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
+        amp_elem_kernel<MODE, true><<<(unsigned)(nbi * dy.o), 256, 0, ctx->stream>>>(e);
         end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
@@ -769,6 +804,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
                                dy.VR, dy.v, dy.vp, 0, ctx->gam[sy].as<double>(), 1));
         }
     }
+    CD_RC(reduce_deps(ctx, prow, pcol, pocc, dx.o, dy.o, dx.VR, dy.VR, dx.v, dy.v, deps_x, deps_y));
     return MSHQC_CD_OK;
 }
 
@@ -787,7 +823,11 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
     const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)(budget / per_i)));
     CD_ALLOC(ctx->W, per_i / 2 * bi, false);
     CD_ALLOC(ctx->amp, per_i / 2 * bi, false);
-    const int64_t tiles_per_i = dy.o * (dx.vp / 32) * (dy.vp / 32);
+    const int64_t npairs = dx.o * dy.o;
+    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.vp + dy.vp + 1)), false);
+    double* prow = ctx->dsum.as<double>();
+    double* pcol = prow + npairs * dx.vp;
+    double* pocc = pcol + npairs * dy.vp;
     for (int i0 = 0; i0 < dx.o; i0 += bi) {
         const int nbi = (int)std::min<int64_t>(bi, dx.o - i0);
         const double* Xb = X.B64.as<double>() + (int64_t)i0 * dx.vp * Mp;
@@ -811,10 +851,10 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
         e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
         e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
         e.A64 = ctx->amp.as<double>();  e.ldA = ldS;
-        e.deps_x = deps_x;  e.deps_y = deps_y;
-        e.partial = partial + (int64_t)i0 * tiles_per_i;
+        e.partial = partial;
+        e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
         begin_stage(ctx, ST_AMP_ELEM);
-        amp_elem_kernel<MODE, false><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
+        amp_elem_kernel<MODE, false><<<(unsigned)(nbi * dy.o), 256, 0, ctx->stream>>>(e);
         end_stage(ctx);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
@@ -841,6 +881,7 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
         }
         end_stage(ctx);
     }
+    CD_RC(reduce_deps(ctx, prow, pcol, pocc, dx.o, dy.o, dx.vp, dy.vp, dx.v, dy.v, deps_x, deps_y));
     return MSHQC_CD_OK;
 }
 
@@ -856,7 +897,7 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
     CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
     CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
-    const int64_t tiles = d.o * d.o * (d.VR / 32) * (d.VR / 32);
+    const int64_t tiles = d.o * d.o;   // one energy per pair (i, j)
     CD_ALLOC(ctx->partial, sizeof(double) * (size_t)tiles, false);
     CD_RC(tc_backward_pass<AMP_RESTRICTED>(ctx, 0, 0, bt, bt, RQ, deps, deps, ctx->partial.as<double>(), 0));
     reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)tiles, ctx->totals.as<double>());
@@ -896,8 +937,7 @@ int gradient_unrestricted(mshqc_cd_ctx* ctx, int precision, double* const dC[2],
     for (int s = 0; s < 2; ++s) CD_CUDA(cudaMemsetAsync(deps[s], 0, sizeof(double) * N, ctx->stream));
     CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
-    const int64_t ra = tc ? da.VR / 32 : da.vp / 32, rb = tc ? db.VR / 32 : db.vp / 32;
-    const int64_t n0 = da.o * da.o * ra * ra, n1 = db.o * db.o * rb * rb, n2 = da.o * db.o * ra * rb;
+    const int64_t n0 = da.o * da.o, n1 = db.o * db.o, n2 = da.o * db.o;   // one energy per pair
     CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(n0 + n1 + n2), false);
     double* part = ctx->partial.as<double>();
     if (tc) {

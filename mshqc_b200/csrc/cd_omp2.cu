@@ -142,7 +142,7 @@ struct OpdmOut {
 // energies to `partial` when it is not null.
 template <int MODE>
 int opdm_pass(mshqc_cd_ctx* ctx, int sx, int sy, double col_coef, double row_coef, const OpdmOut& out,
-              double* partial, double* deps_scratch) {
+              double* partial) {
     SpinState& X = ctx->spin[sx];
     SpinState& Y = ctx->spin[sy];
     const int64_t N = ctx->N, Mp = ctx->Mp;
@@ -156,7 +156,11 @@ int opdm_pass(mshqc_cd_ctx* ctx, int sx, int sy, double col_coef, double row_coe
     const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)(budget / per_i)));
     CD_ALLOC(ctx->W, per_i / 2 * bi, false);
     CD_ALLOC(ctx->amp, per_i / 2 * bi, false);
-    const int64_t tiles_per_i = oy * (vpx / 32) * (vpy / 32);
+    if (!partial) {
+        // energies of this pass are not needed: throw-away slots, one per pair
+        CD_ALLOC(ctx->pair_sum, sizeof(double) * (size_t)(ox * oy), false);
+        partial = ctx->pair_sum.as<double>();
+    }
     for (int i0 = 0; i0 < ox; i0 += bi) {
         const int nbi = (int)std::min<int64_t>(bi, ox - i0);
         const int64_t R = (int64_t)nbi * vpx;
@@ -178,15 +182,8 @@ int opdm_pass(mshqc_cd_ctx* ctx, int sx, int sy, double col_coef, double row_coe
         e.eox = X.eps.as<double>();  e.evx = e.eox + ox;
         e.eoy = Y.eps.as<double>();  e.evy = e.eoy + oy;
         e.A64 = ctx->amp.as<double>();  e.ldA = ldS;
-        e.deps_x = deps_scratch;  e.deps_y = deps_scratch + N;
-        if (partial) {
-            e.partial = partial + (int64_t)i0 * tiles_per_i;
-        } else {
-            // energies of this pass are not needed: one throw-away slot per tile
-            CD_ALLOC(ctx->pair_sum, sizeof(double) * (size_t)(nbi * tiles_per_i), false);
-            e.partial = ctx->pair_sum.as<double>();
-        }
-        amp_elem_kernel<MODE, false><<<(unsigned)(nbi * tiles_per_i), 256, 0, ctx->stream>>>(e);
+        e.partial = partial;   // no dE/de here: prow, pcol, pocc stay null
+        amp_elem_kernel<MODE, false><<<(unsigned)(nbi * oy), 256, 0, ctx->stream>>>(e);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
         // column Gram: Gvv_x[a][b] += c * sum_K A[(i,a)][K] A[(i,b)][K], one GEMM per i
@@ -271,18 +268,16 @@ int omp2_pieces_device(mshqc_cd_ctx* ctx, const double* const Pref[2], Omp2Buffe
     // OPDM blocks start at zero
     CD_CUDA(cudaMemsetAsync(b.Goo[0], 0, sizeof(double) * (size_t)(o0 * o0 + o1 * o1 + vp0 * vp0 + vp1 * vp1),
                             ctx->stream));
-    CD_CUDA(cudaMemsetAsync(b.deps, 0, sizeof(double) * 2 * N, ctx->stream));
     CD_ALLOC(ctx->totals, sizeof(double) * 16, false);
-    const int64_t n0 = o0 * o0 * (vp0 / 32) * (vp0 / 32), n1 = o1 * o1 * (vp1 / 32) * (vp1 / 32);
-    const int64_t n2 = o0 * o1 * (vp0 / 32) * (vp1 / 32);
+    const int64_t n0 = o0 * o0, n1 = o1 * o1, n2 = o0 * o1;   // one energy per pair
     CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(n0 + n1 + n2), false);
     double* part = ctx->partial.as<double>();
     OpdmOut out{{b.Goo[0], b.Goo[1]}, {b.Gvv[0], b.Gvv[1]}};
     begin_stage(ctx, ST_AMPLITUDE);
-    CD_RC(opdm_pass<AMP_SAME_SPIN>(ctx, 0, 0, 0.5, -0.5, out, part, b.deps));
-    CD_RC(opdm_pass<AMP_SAME_SPIN>(ctx, 1, 1, 0.5, -0.5, out, part + n0, b.deps));
-    CD_RC(opdm_pass<AMP_OPPOSITE_SPIN>(ctx, 0, 1, 1.0, -1.0, out, part + n0 + n1, b.deps));
-    CD_RC(opdm_pass<AMP_OPPOSITE_SPIN>(ctx, 1, 0, 1.0, -1.0, out, nullptr, b.deps));
+    CD_RC(opdm_pass<AMP_SAME_SPIN>(ctx, 0, 0, 0.5, -0.5, out, part));
+    CD_RC(opdm_pass<AMP_SAME_SPIN>(ctx, 1, 1, 0.5, -0.5, out, part + n0));
+    CD_RC(opdm_pass<AMP_OPPOSITE_SPIN>(ctx, 0, 1, 1.0, -1.0, out, part + n0 + n1));
+    CD_RC(opdm_pass<AMP_OPPOSITE_SPIN>(ctx, 1, 0, 1.0, -1.0, out, nullptr));
     end_stage(ctx);
     const int64_t offs[3] = {0, n0, n0 + n1}, cnt[3] = {n0, n1, n2};
     for (int k = 0; k < 3; ++k) {
@@ -454,6 +449,9 @@ int require_omp2_inputs(mshqc_cd_ctx* ctx) {
     if (!ctx->spin[0].set || !ctx->spin[1].set)
         return set_error(MSHQC_CD_ERR_STATE, "OMP2 needs alpha and beta orbitals (set both; equal for RHF)");
     if (!ctx->H_set) return set_error(MSHQC_CD_ERR_STATE, "core Hamiltonian not set");
+    if (ctx->L_gen)
+        return set_error(MSHQC_CD_ERR_UNSUPPORTED,
+                         "OMP2 needs stored Cholesky vectors (mshqc_cd_set_vectors), not generated ones");
     return MSHQC_CD_OK;
 }
 

@@ -171,6 +171,66 @@ def make_vectors_device(N: int, M: int, seed: int, sigma: float, device, chunk: 
     return L
 
 
+_PHILOX_M = (np.uint64(0xD2511F53), np.uint64(0xCD9E8D57))
+_PHILOX_W = (np.uint32(0x9E3779B9), np.uint32(0xBB67AE85))
+_MASK32 = np.uint64(0xFFFFFFFF)
+
+
+def philox4x32_10(ctr: np.ndarray, seed: int) -> tuple:
+    """Philox4x32-10 (Salmon et al., SC 2011) of the 64-bit counters `ctr`
+    (words (ctr_lo, ctr_hi, 0, 0)) under key `seed`; four uint32 arrays."""
+    ctr = np.asarray(ctr, dtype=np.uint64)
+    c0 = (ctr & _MASK32).astype(np.uint32)
+    c1 = (ctr >> np.uint64(32)).astype(np.uint32)
+    return philox4x32_10_words(c0, c1, np.zeros_like(c0), np.zeros_like(c0),
+                               seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
+
+
+def philox4x32_10_words(c0, c1, c2, c3, key0: int, key1: int) -> tuple:
+    """The ten Philox4x32 rounds on counter words c0..c3 (uint32 arrays) and
+    key (key0, key1): per round (hi0, lo0) = M0 c0, (hi1, lo1) = M1 c2,
+    c <- (hi1 ^ c1 ^ k0, lo1, hi0 ^ c3 ^ k1, lo0), then the key grows by the
+    Weyl constants."""
+    c0, c1, c2, c3 = (np.asarray(c, dtype=np.uint32) for c in (c0, c1, c2, c3))
+    k0 = np.uint32(key0)
+    k1 = np.uint32(key1)
+    with np.errstate(over="ignore"):
+        for _ in range(10):
+            p0 = _PHILOX_M[0] * c0.astype(np.uint64)
+            p1 = _PHILOX_M[1] * c2.astype(np.uint64)
+            hi0, lo0 = (p0 >> np.uint64(32)).astype(np.uint32), (p0 & _MASK32).astype(np.uint32)
+            hi1, lo1 = (p1 >> np.uint64(32)).astype(np.uint32), (p1 & _MASK32).astype(np.uint32)
+            c0, c1, c2, c3 = hi1 ^ c1 ^ k0, lo1, hi0 ^ c3 ^ k1, lo0
+            k0 = np.uint32(k0 + _PHILOX_W[0])
+            k1 = np.uint32(k1 + _PHILOX_W[1])
+    return c0, c1, c2, c3
+
+
+def philox_normal(ctr: np.ndarray, seed: int) -> np.ndarray:
+    """Box-Muller standard normal of one Philox block per counter."""
+    c0, c1, c2, c3 = philox4x32_10(ctr, seed)
+    a = (c0.astype(np.uint64) << np.uint64(32)) | c1.astype(np.uint64)
+    b = (c2.astype(np.uint64) << np.uint64(32)) | c3.astype(np.uint64)
+    u1 = ((a >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    u2 = ((b >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586 * u2)
+
+
+def make_vectors_philox(N: int, M: int, seed: int, sigma: float = 1.0) -> np.ndarray:
+    """The recipe as the library's device generator draws it
+    (mshqc_cd_gen_vectors): X^Q_{mu nu} = philox_normal((Q N + mu) N + nu),
+    L^Q = sigma 10^(-6Q/M) (X + X^T)/2.  (M, N*N) float64; for small sizes."""
+    s = scale_factors(M) * sigma
+    L = np.empty((M, N * N), dtype=np.float64)
+    mu = np.arange(N, dtype=np.uint64)[:, None]
+    nu = np.arange(N, dtype=np.uint64)[None, :]
+    for q in range(M):
+        base = np.uint64(q) * np.uint64(N)
+        Z = philox_normal((base + mu) * np.uint64(N) + nu, seed)
+        L[q] = (s[q] * (0.5 * (Z + Z.T))).reshape(N * N)
+    return L
+
+
 def make_orbitals(N: int, nocc: int, seed: int) -> SpinOrbitals:
     rng = np.random.default_rng(seed)
     return SpinOrbitals(_orthogonal(rng, N), _orbital_energies(rng, N, nocc), nocc)
