@@ -17,8 +17,10 @@
 // Gamma = amplitude x B is formed afterwards by a GEMM with K = (j, b); this
 // pass writes the amplitude operand of that GEMM: BF16 hi/lo in the blocked
 // K-major layout of the tensor-core Gamma kernel (SPLIT), or FP64 row-major
-// [(i - i0, a)][(j, b)] for the FP64 GEMM.  OPPOSITE_SPIN with SPLIT also
-// writes the transposed operand [(j, b)][(i - i0, a)] for Gamma_beta.
+// [(i - i0, a)][(j, b)] for the FP64 GEMM.  With SPLIT it can also write the
+// transposed operand [(j, b)][(i - i0, a)]: Gamma_beta of the opposite-spin
+// pass, or, for the symmetric modes (t^{ji}_{ba} = t^{ij}_{ab}), the rows j of
+// a block pair (I, J) whose mirror (J, I) is not computed.
 // One CTA of 256 threads takes one pair (i, j) and walks its 32 x 32 tiles of
 // (a, b), column block outer; the pair's energy, its row sums
 // sum_b r (per a), column sums sum_a r (per b) and total sum r go to per-pair
@@ -42,12 +44,14 @@ struct AmpElemArgs {
     int rsx;                // rows per occupied i in S and in the output (multiple of 32)
     int csy;                // columns per occupied j in S
     int ksy;                // output K per occupied j (multiple of 32, <= csy)
-    int ox, oy, vx, vy, i0, nbi;
+    int ox, oy, vx, vy, i0, nbi;   // oy: all column orbitals (pair index i * oy + j)
+    int j0, nbj;            // the column orbitals of this block: j0 .. j0 + nbj - 1
+    double wgt;             // weight of the pair sums (2 when the mirror block (J, I) is skipped)
     const double* eox; const double* evx;   // energies of the row spin
     const double* eoy; const double* evy;   // of the column spin
-    uint16_t* Ahi; uint16_t* Alo; long long RA;   // SPLIT: rows R = ii*rsx + a, K = j*ksy + b
-    uint16_t* Thi; uint16_t* Tlo; long long RT;   // SPLIT, OPPOSITE_SPIN: rows j*ksy + b, K = ii*rsx + a
-    double* A64; long long ldA;                   // FP64: [R][K]
+    uint16_t* Ahi; uint16_t* Alo; long long RA;   // SPLIT: rows R = ii*rsx + a, K = jj*ksy + b
+    uint16_t* Thi; uint16_t* Tlo; long long RT;   // SPLIT, optional transpose: rows jj*ksy + b, K = ii*rsx + a
+    double* A64; long long ldA;                   // FP64: [R][K], K = jj*ksy + b
     double* partial;        // [ox * oy] energy of each pair (i, j), i over all row orbitals
     double* prow;           // [ox * oy][rsx] sum_b r per pair and row a (or null)
     double* pcol;           // [ox * oy][ksy] sum_a r per pair and column b (or null)
@@ -87,7 +91,8 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
     __shared__ double red_e[8], red_r[8];
     const TS* S = static_cast<const TS*>(p.S);
     const int ta = p.rsx / 32, tb = p.ksy / 32;
-    const int ii = (int)(blockIdx.x / p.oy), j = (int)(blockIdx.x % p.oy), i = p.i0 + ii;
+    const int ii = (int)(blockIdx.x / p.nbj), jj = (int)(blockIdx.x % p.nbj);
+    const int i = p.i0 + ii, j = p.j0 + jj;
     const long long pair = (long long)i * p.oy + j;          // over all occupied rows
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
     const double eij = p.eox[i] + p.eoy[j];
@@ -101,9 +106,9 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
             const int a0 = xb * 32;
 #pragma unroll
             for (int r = ty; r < 32; r += 8) {
-                Vt[r][tx] = S[((long long)ii * p.rsx + a0 + r) * p.ldS + (long long)j * p.csy + b0 + tx];
+                Vt[r][tx] = S[((long long)ii * p.rsx + a0 + r) * p.ldS + (long long)jj * p.csy + b0 + tx];
                 if (MODE != AMP_OPPOSITE_SPIN)   // (ib|ja): rows (i, b), columns (j, a)
-                    Wt[r][tx] = S[((long long)ii * p.rsx + b0 + r) * p.ldS + (long long)j * p.csy + a0 + tx];
+                    Wt[r][tx] = S[((long long)ii * p.rsx + b0 + r) * p.ldS + (long long)jj * p.csy + a0 + tx];
             }
             __syncthreads();
 #pragma unroll
@@ -142,8 +147,8 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
 #pragma unroll
                 for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
                 // row a is always summed by lane 0 of warp ty: single writer, program order
-                if (prow && tx == 0) prow[a] = (yb == 0 ? 0.0 : prow[a]) + rs;
-                if (!SPLIT) p.A64[((long long)ii * p.rsx + a) * p.ldA + (long long)j * p.ksy + b] = amp;
+                if (prow && tx == 0) prow[a] = (yb == 0 ? 0.0 : prow[a]) + p.wgt * rs;
+                if (!SPLIT) p.A64[((long long)ii * p.rsx + a) * p.ldA + (long long)jj * p.ksy + b] = amp;
             }
             if (SPLIT) {
                 __syncthreads();
@@ -151,13 +156,13 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                 if (threadIdx.x < 128) {
                     const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
                     const long long R = (long long)ii * p.rsx + a0 + r;
-                    const long long kc = (long long)j * p.ksy + b0 + g * 8;
+                    const long long kc = (long long)jj * p.ksy + b0 + g * 8;
                     const long long off = amp_detail::blocked_offset(R, kc, p.RA);
                     amp_detail::store_hilo8(&T[r][g * 8], p.Ahi + off, p.Alo + off);
-                } else if (MODE == AMP_OPPOSITE_SPIN) {
+                } else if (p.Thi) {
                     const int w = threadIdx.x - 128;
                     const int r = w >> 2, g = w & 3;   // r: b offset, g: group of 8 a
-                    const long long R = (long long)j * p.ksy + b0 + r;
+                    const long long R = (long long)jj * p.ksy + b0 + r;
                     const long long kc = (long long)ii * p.rsx + a0 + g * 8;
                     const long long off = amp_detail::blocked_offset(R, kc, p.RT);
                     double col[8];
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                 double c = 0.0;
 #pragma unroll
                 for (int w = 0; w < 8; ++w) c += colpart[w][tx];
-                pcol[b0 + tx] = c;
+                pcol[b0 + tx] = p.wgt * c;
             }
             __syncthreads();
         }
@@ -196,8 +201,8 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
             e += red_e[w];
             r += red_r[w];
         }
-        p.partial[pair] = e;
-        if (p.pocc) p.pocc[pair] = r;
+        p.partial[pair] = p.wgt * e;
+        if (p.pocc) p.pocc[pair] = p.wgt * r;
     }
 }
 

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -717,91 +718,119 @@ int reduce_deps(mshqc_cd_ctx* ctx, const double* prow, const double* pcol, const
     return MSHQC_CD_OK;
 }
 
-// One mixed-precision backward pass: the occupied rows i of spin sx in
-// blocks against every j of spin sy.  Per block: (ia|jb) tiles on the tensor
-// cores (exact fixed point, FP32 staging), the element-wise amplitude pass,
-// Gamma_sx (+)= amplitudes x B_sy and, for the opposite-spin pass,
-// Gamma_sy += amplitudes^T x B_sx.  Energy partials go to `partial`
-// (ox * oy * (VRx/32) * (VRy/32) tiles).
+// One mixed-precision backward pass over block pairs (I, J): rows i in I of
+// spin sx, columns j in J of spin sy.  Per block pair: (ia|jb) tiles on the
+// tensor cores (exact fixed point, FP32 staging), the element-wise amplitude
+// pass, Gamma_sx[I] += amplitudes x B_sy[J] and, when `mirror`, the transposed
+// amplitudes update Gamma_sy[J] += amplitudes^T x B_sx[I].
+//  * same spin / restricted: blocks of b orbitals, I <= J only.  The amplitude
+//    of pair (j, i) is the transpose of that of (i, j) (t^{ji}_{ba} =
+//    t^{ij}_{ab}), so off-diagonal pairs are computed once and count twice;
+//    this halves the integral tiles and the element-wise pass.
+//  * opposite spin: row blocks I against all beta columns (no symmetry).
+// Energies go to `partial` (ox * oy, one per ordered pair, zero where a
+// mirrored pair stands in), dE/de to deps_x / deps_y.
 template <int MODE>
 int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const btx[2],
                      const uint16_t* const bty[2], int64_t RQ, double* deps_x, double* deps_y,
-                     double* partial, int accumulate_x) {
+                     double* partial) {
+    constexpr bool kSym = MODE != AMP_OPPOSITE_SPIN;
     SpinState& X = ctx->spin[sx];
     SpinState& Y = ctx->spin[sy];
     const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
-    const int64_t Mp = ctx->Mp, KA = dy.o * dy.VR;
+    const int64_t Mp = ctx->Mp;
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_i_amp = sizeof(uint16_t) * (size_t)dx.VR * KA;
-    const size_t per_i_s = sizeof(float) * (size_t)dx.VR * (size_t)(dy.o * dy.VS);
-    const size_t per_i_t = MODE == AMP_OPPOSITE_SPIN ? per_i_amp : 0;
-    const size_t per_i = 2 * per_i_amp + per_i_s + 2 * per_i_t;
-    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 3, size_t(40) << 30));
-    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)(budget / per_i)));
-    CD_ALLOC(ctx->amp, per_i_amp * bi, false);
-    CD_ALLOC(ctx->amp2, per_i_amp * bi, false);
-    CD_ALLOC(ctx->W, per_i_s * bi, false);
-    if (MODE == AMP_OPPOSITE_SPIN) {
-        CD_ALLOC(ctx->ampT, per_i_t * bi, false);
-        CD_ALLOC(ctx->ampT2, per_i_t * bi, false);
+    const size_t budget = std::min<size_t>(free_b / 3, size_t(40) << 30);
+    // block sizes: rows bI, columns bJ (all of them for the opposite spin)
+    int64_t bI, bJ;
+    if (kSym) {
+        const double per_b2 = (double)dx.VR * (4.0 * dy.VS + 8.0 * dy.VR);   // S + A1 + A2 per (i, j)
+        bI = bJ = std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)std::sqrt((double)budget / per_b2)));
+    } else {
+        const double per_i = (double)dx.VR * dy.o * (4.0 * dy.VS + 8.0 * dy.VR);
+        bI = std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)((double)budget / per_i)));
+        bJ = dy.o;
     }
+    // MSHQC_CD_BWD_BLOCK (occupied orbitals per block) overrides the choice
+    if (const char* env = std::getenv("MSHQC_CD_BWD_BLOCK")) {
+        const long long b = std::atoll(env);
+        if (b > 0) {
+            bI = std::min<int64_t>(dx.o, b);
+            if (kSym) bJ = bI;
+        }
+    }
+    const size_t n_amp = sizeof(uint16_t) * (size_t)(bI * dx.VR) * (size_t)(bJ * dy.VR);
+    CD_ALLOC(ctx->amp, n_amp, false);
+    CD_ALLOC(ctx->amp2, n_amp, false);
+    CD_ALLOC(ctx->ampT, n_amp, false);
+    CD_ALLOC(ctx->ampT2, n_amp, false);
+    CD_ALLOC(ctx->W, sizeof(float) * (size_t)(bI * dx.VR) * (size_t)(bJ * dy.VS), false);
     const int64_t npairs = dx.o * dy.o;
-    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.VR + dy.VR + 1)), false);
+    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.VR + dy.VR + 1)), true);
+    CD_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * (size_t)npairs, ctx->stream));
     double* prow = ctx->dsum.as<double>();
     double* pcol = prow + npairs * dx.VR;
     double* pocc = pcol + npairs * dy.VR;
     const size_t vsm = vtile_tc::SMEM_BYTES;
     CD_CUDA(cudaFuncSetAttribute(vtile_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
-    for (int i0 = 0; i0 < dx.o; i0 += bi) {
-        const int nbi = (int)std::min<int64_t>(bi, dx.o - i0);
-        VtileArgs a{};
-        a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
-        a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
-        a.ex = X.expo.as<int>();  a.ey = Y.expo.as<int>();
-        a.diag = sx == sy ? X.diag.as<double>() : nullptr;
-        a.rows_x = (int)X.vp16;  a.rows_y = (int)Y.vp16;
-        a.nqc = (int)(Mp / 16);
-        a.oy = (int)dy.o;  a.vx = (int)dx.v;  a.vy = (int)dy.v;
-        a.VR = (int)dx.VR;  a.i0 = i0;  a.nbi = nbi;
-        a.nbx = (int)(dx.VR / 128);  a.nby = (int)dy.nby;  a.VS = (int)dy.VS;
-        a.S = ctx->W.as<float>();
-        a.err = ctx->flag.as<int>();
-        const int64_t vunits = (int64_t)nbi * dy.o * a.nbx * a.nby;
-        const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
-        begin_stage(ctx, ST_AMPLITUDE);
-        vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
-        end_stage(ctx);
-        CD_CUDA(cudaGetLastError());
-        ctx->launches++;
-        AmpElemArgs e{};
-        e.S = ctx->W.as<float>();
-        e.ldS = dy.o * dy.VS;
-        e.rsx = (int)dx.VR;  e.csy = (int)dy.VS;  e.ksy = (int)dy.VR;
-        e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
-        e.i0 = i0;  e.nbi = nbi;
-        e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
-        e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
-        e.Ahi = ctx->amp.as<uint16_t>();  e.Alo = ctx->amp2.as<uint16_t>();
-        e.RA = (long long)bi * dx.VR;
-        if (MODE == AMP_OPPOSITE_SPIN) {
-            e.Thi = ctx->ampT.as<uint16_t>();  e.Tlo = ctx->ampT2.as<uint16_t>();
-            e.RT = (long long)KA;
-        }
-        e.partial = partial;
-        e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
-        begin_stage(ctx, ST_AMP_ELEM);
-        amp_elem_kernel<MODE, true><<<(unsigned)(nbi * dy.o), 256, 0, ctx->stream>>>(e);
-        end_stage(ctx);
-        CD_CUDA(cudaGetLastError());
-        ctx->launches++;
-        CD_RC(launch_gamma(ctx, e.Ahi, e.Alo, e.RA, bty[0], bty[1], RQ, KA, (int64_t)nbi * dx.VR, dx.VR, dx.v,
-                           dx.vp, i0, ctx->gam[sx].as<double>(), accumulate_x));
-        if (MODE == AMP_OPPOSITE_SPIN) {
-            // K range of this block inside the transposed B of spin sx
-            const size_t k0 = (size_t)i0 * dx.VR * RQ;
-            CD_RC(launch_gamma(ctx, e.Thi, e.Tlo, KA, btx[0] + k0, btx[1] + k0, RQ, (int64_t)nbi * dx.VR, KA,
-                               dy.VR, dy.v, dy.vp, 0, ctx->gam[sy].as<double>(), 1));
+    for (int64_t I0 = 0; I0 < dx.o; I0 += bI) {
+        const int nI = (int)std::min<int64_t>(bI, dx.o - I0);
+        for (int64_t J0 = kSym ? I0 : 0; J0 < dy.o; J0 += bJ) {
+            const int nJ = (int)std::min<int64_t>(bJ, dy.o - J0);
+            const bool mirror = !kSym || J0 != I0;
+            VtileArgs a{};
+            a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
+            a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
+            a.ex = X.expo.as<int>();  a.ey = Y.expo.as<int>();
+            a.diag = sx == sy ? X.diag.as<double>() : nullptr;
+            a.rows_x = (int)X.vp16;  a.rows_y = (int)Y.vp16;
+            a.nqc = (int)(Mp / 16);
+            a.j0 = (int)J0;  a.nbj = nJ;
+            a.vx = (int)dx.v;  a.vy = (int)dy.v;
+            a.VR = (int)dx.VR;  a.i0 = (int)I0;  a.nbi = nI;
+            a.nbx = (int)(dx.VR / 128);  a.nby = (int)dy.nby;  a.VS = (int)dy.VS;
+            a.S = ctx->W.as<float>();
+            a.err = ctx->flag.as<int>();
+            const int64_t vunits = (int64_t)nI * nJ * a.nbx * a.nby;
+            const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
+            begin_stage(ctx, ST_AMPLITUDE);
+            vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
+            end_stage(ctx);
+            CD_CUDA(cudaGetLastError());
+            ctx->launches++;
+            AmpElemArgs e{};
+            e.S = ctx->W.as<float>();
+            e.ldS = (long long)nJ * dy.VS;
+            e.rsx = (int)dx.VR;  e.csy = (int)dy.VS;  e.ksy = (int)dy.VR;
+            e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
+            e.i0 = (int)I0;  e.nbi = nI;  e.j0 = (int)J0;  e.nbj = nJ;
+            e.wgt = (kSym && mirror) ? 2.0 : 1.0;
+            e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
+            e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
+            e.Ahi = ctx->amp.as<uint16_t>();  e.Alo = ctx->amp2.as<uint16_t>();
+            e.RA = (long long)bI * dx.VR;
+            if (mirror) {
+                e.Thi = ctx->ampT.as<uint16_t>();  e.Tlo = ctx->ampT2.as<uint16_t>();
+                e.RT = (long long)bJ * dy.VR;
+            }
+            e.partial = partial;
+            e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
+            begin_stage(ctx, ST_AMP_ELEM);
+            amp_elem_kernel<MODE, true><<<(unsigned)(nI * nJ), 256, 0, ctx->stream>>>(e);
+            end_stage(ctx);
+            CD_CUDA(cudaGetLastError());
+            ctx->launches++;
+            // Gamma_sx[I] += A x B_sy[J]  (K range of J inside the transposed B of spin sy)
+            const size_t kJ = (size_t)J0 * dy.VR * RQ, kI = (size_t)I0 * dx.VR * RQ;
+            CD_RC(launch_gamma(ctx, e.Ahi, e.Alo, e.RA, bty[0] + kJ, bty[1] + kJ, RQ, (int64_t)nJ * dy.VR,
+                               (int64_t)nI * dx.VR, dx.VR, dx.v, dx.vp, (int)I0, ctx->gam[sx].as<double>(), 1));
+            if (mirror) {
+                // Gamma_sy[J] += A^T x B_sx[I]
+                CD_RC(launch_gamma(ctx, e.Thi, e.Tlo, e.RT, btx[0] + kI, btx[1] + kI, RQ, (int64_t)nI * dx.VR,
+                                   (int64_t)nJ * dy.VR, dy.VR, dy.v, dy.vp, (int)J0, ctx->gam[sy].as<double>(),
+                                   1));
+            }
         }
     }
     CD_RC(reduce_deps(ctx, prow, pcol, pocc, dx.o, dy.o, dx.VR, dy.VR, dx.v, dy.v, deps_x, deps_y));
@@ -847,7 +876,7 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
         e.ldS = ldS;
         e.rsx = (int)dx.vp;  e.csy = (int)dy.vp;  e.ksy = (int)dy.vp;
         e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
-        e.i0 = i0;  e.nbi = nbi;
+        e.i0 = i0;  e.nbi = nbi;  e.j0 = 0;  e.nbj = (int)dy.o;  e.wgt = 1.0;
         e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
         e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
         e.A64 = ctx->amp.as<double>();  e.ldA = ldS;
@@ -899,7 +928,7 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
     const int64_t tiles = d.o * d.o;   // one energy per pair (i, j)
     CD_ALLOC(ctx->partial, sizeof(double) * (size_t)tiles, false);
-    CD_RC(tc_backward_pass<AMP_RESTRICTED>(ctx, 0, 0, bt, bt, RQ, deps, deps, ctx->partial.as<double>(), 0));
+    CD_RC(tc_backward_pass<AMP_RESTRICTED>(ctx, 0, 0, bt, bt, RQ, deps, deps, ctx->partial.as<double>()));
     reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)tiles, ctx->totals.as<double>());
     CD_CUDA(cudaGetLastError());
     ctx->launches++;
@@ -941,9 +970,9 @@ int gradient_unrestricted(mshqc_cd_ctx* ctx, int precision, double* const dC[2],
     CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(n0 + n1 + n2), false);
     double* part = ctx->partial.as<double>();
     if (tc) {
-        CD_RC(tc_backward_pass<AMP_SAME_SPIN>(ctx, 0, 0, bta, bta, RQ, deps[0], deps[0], part, 1));
-        CD_RC(tc_backward_pass<AMP_SAME_SPIN>(ctx, 1, 1, btb, btb, RQ, deps[1], deps[1], part + n0, 1));
-        CD_RC(tc_backward_pass<AMP_OPPOSITE_SPIN>(ctx, 0, 1, bta, btb, RQ, deps[0], deps[1], part + n0 + n1, 1));
+        CD_RC(tc_backward_pass<AMP_SAME_SPIN>(ctx, 0, 0, bta, bta, RQ, deps[0], deps[0], part));
+        CD_RC(tc_backward_pass<AMP_SAME_SPIN>(ctx, 1, 1, btb, btb, RQ, deps[1], deps[1], part + n0));
+        CD_RC(tc_backward_pass<AMP_OPPOSITE_SPIN>(ctx, 0, 1, bta, btb, RQ, deps[0], deps[1], part + n0 + n1));
     } else {
         CD_RC(f64_backward_pass<AMP_SAME_SPIN>(ctx, 0, 0, deps[0], deps[0], part));
         CD_RC(f64_backward_pass<AMP_SAME_SPIN>(ctx, 1, 1, deps[1], deps[1], part + n0));

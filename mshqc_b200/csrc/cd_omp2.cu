@@ -178,7 +178,7 @@ int opdm_pass(mshqc_cd_ctx* ctx, int sx, int sy, double col_coef, double row_coe
         e.ldS = ldS;
         e.rsx = (int)vpx;  e.csy = (int)vpy;  e.ksy = (int)vpy;
         e.ox = (int)ox;  e.oy = (int)oy;  e.vx = (int)vx;  e.vy = (int)vy;
-        e.i0 = i0;  e.nbi = nbi;
+        e.i0 = i0;  e.nbi = nbi;  e.j0 = 0;  e.nbj = (int)oy;  e.wgt = 1.0;
         e.eox = X.eps.as<double>();  e.evx = e.eox + ox;
         e.eoy = Y.eps.as<double>();  e.evy = e.eoy + oy;
         e.A64 = ctx->amp.as<double>();  e.ldA = ldS;

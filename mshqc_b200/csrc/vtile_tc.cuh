@@ -2,7 +2,8 @@
 //
 //   S[(i - i0, a)][(j, b)] = (ia|jb) = sum_Q X^Q_ia Y^Q_jb     (FP32)
 //
-// for the occupied rows i of one block and all j, every tile computed once;
+// for the occupied rows i of one block and the columns j of another (or all
+// j), every tile computed once;
 // X and Y are the MO vectors of one spin (restricted, same spin) or of the
 // two spins (opposite spin: X alpha, Y beta).
 // Operands are the exact fixed-point hi/lo of split_bf16.cuh in the blocked
@@ -12,7 +13,7 @@
 //   (ia|jb) = u_ia u_jb (hh + x / 256)
 // in FP64, substitutes the exact (ia|ia) for i = j, a = b when X = Y, and
 // stores it rounded to FP32 into the row-major staging matrix S (row length
-// oy * VS).  amp_elem.cuh turns S into amplitudes.
+// nbj * VS).  amp_elem.cuh turns S into amplitudes.
 //
 // Warp roles (192 threads): warp 0 producer, warp 1 MMA issuer and TMEM
 // owner, warps 2..5 epilogue.  Waits are bounded as in pair_energy_tc.cuh.
@@ -32,10 +33,11 @@ struct VtileArgs {
     const double* diag;                         // exact (ia|ia) [o][rows_x] when X = Y, else null
     int rows_x, rows_y;     // allocated rows per occupied orbital (operand layouts)
     int nqc;                // 16-wide Q chunks
-    int oy, vx, vy, VR, i0, nbi;   // VR: staging rows per orbital i (nbx * 128)
+    int j0, nbj;            // column orbitals j0 .. j0 + nbj - 1
+    int vx, vy, VR, i0, nbi;       // VR: staging rows per orbital i (nbx * 128)
     int nbx, nby;           // row blocks (128) per orbital i, column ranges (256) per orbital j
     int VS;                 // staging columns per orbital j (nby * 256)
-    float* S;               // staging [nbi * VR][oy * VS]
+    float* S;               // staging [nbi * VR][nbj * VS]
     int* err;
 };
 
@@ -88,7 +90,7 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
 
     // unit u -> (ii, j, x, y): pair-major so that concurrent CTAs share slabs
     const long long per_pair = (long long)p.nbx * p.nby;
-    const long long units = (long long)p.nbi * p.oy * per_pair;
+    const long long units = (long long)p.nbi * p.nbj * per_pair;
     const long long first = blockIdx.x, step = gridDim.x;
     const int nk = p.nqc;
 
@@ -97,7 +99,7 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
             uint32_t stage = 0, phase = 0, fill_phase = 0, filled = 0;
             for (long long u = first; u < units && !*abort_flag; u += step) {
                 const long long pr = u / per_pair, bb = u % per_pair;
-                const int i = p.i0 + (int)(pr / p.oy), j = (int)(pr % p.oy);
+                const int i = p.i0 + (int)(pr / p.nbj), j = p.j0 + (int)(pr % p.nbj);
                 const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
                 const size_t rx = p.rows_x, ry = p.rows_y;
                 const uint16_t* ah = p.Xhi + (size_t)i * p.nqc * rx * 16 + (size_t)x * BM * 16;
@@ -177,11 +179,11 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
         const int q = warp & 3;
         const int row = q * 32 + lane;
         const int etid = threadIdx.x - 64;
-        const long long ldS = (long long)p.oy * p.VS;
+        const long long ldS = (long long)p.nbj * p.VS;
         uint32_t acc_phase = 0;
         for (long long u = first; u < units; u += step) {
             const long long pr = u / per_pair, bb = u % per_pair;
-            const int ii = (int)(pr / p.oy), j = (int)(pr % p.oy), i = p.i0 + ii;
+            const int ii = (int)(pr / p.nbj), jj = (int)(pr % p.nbj), i = p.i0 + ii, j = p.j0 + jj;
             const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
             const int a = x * BM + row, b0 = y * BN;
             for (int c = etid; c < BN; c += 128) {
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
             const double rs = arow ? pow2d(p.ex[(size_t)i * p.rows_x + a] - kFixedHiBits) : 0.0;
             const int dcol = (p.diag && arow && i == j && a >= b0 && a < b0 + BN) ? a - b0 : -1;
             const double dg = dcol >= 0 ? p.diag[(size_t)i * p.rows_x + a] : 0.0;
-            float* dst = p.S + ((long long)ii * p.VR + a) * ldS + (long long)j * p.VS + b0;
+            float* dst = p.S + ((long long)ii * p.VR + a) * ldS + (long long)jj * p.VS + b0;
             const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
             float amax = 0.0f;   // integer accumulators stay exact below 2^24
 #pragma unroll 1

@@ -178,3 +178,36 @@ def test_unrestricted_mixed_gradient_vs_fp64(ctx, N, oa, ob, M, seed):
         assert abs(g3.energy[key] - g64.energy[key]) <= 1e-6, key
     for x, y in ((g3.dC_a, g64.dC_a), (g3.dC_b, g64.dC_b), (g3.deps_a, g64.deps_a), (g3.deps_b, g64.deps_b)):
         assert np.max(np.abs(x - y)) <= 1e-6, np.max(np.abs(x - y))
+
+
+# Block pairs: the mixed backward splits the occupied orbitals into blocks
+# and, for the restricted and same-spin passes, computes only block pairs
+# I <= J (the (j, i) amplitudes are the transposes of the (i, j) ones).
+# Small blocks force several block pairs, mirrored ones included.
+@pytest.mark.parametrize("block", ["3", "5"])
+def test_restricted_mixed_gradient_block_pairs(ctx, monkeypatch, block):
+    N, o, M = 120, 13, 280
+    inp = twin(N, o, M, seed=31)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    g64 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
+    one = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
+    monkeypatch.setenv("MSHQC_CD_BWD_BLOCK", block)
+    g3 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
+    assert abs(g3.energy["total"] - g64.energy["total"]) <= 1e-6
+    assert abs(g3.energy["total"] - one.energy["total"]) <= 1e-9
+    assert np.max(np.abs(g3.dC_a - g64.dC_a)) <= 1e-6
+    assert np.max(np.abs(g3.deps_a - g64.deps_a)) <= 1e-6
+    assert np.max(np.abs(g3.dC_a - one.dC_a)) <= 1e-7
+
+
+def test_unrestricted_mixed_gradient_block_pairs(ctx, monkeypatch):
+    inp = twin(100, 11, 240, seed=33, nocc_beta=9)
+    set_unrestricted(ctx, inp)
+    g64 = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP64)
+    monkeypatch.setenv("MSHQC_CD_BWD_BLOCK", "4")
+    g3 = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP16X3)
+    for key in ("ss_aa", "ss_bb", "os", "total"):
+        assert abs(g3.energy[key] - g64.energy[key]) <= 1e-6, key
+    for x, y in ((g3.dC_a, g64.dC_a), (g3.dC_b, g64.dC_b), (g3.deps_a, g64.deps_a), (g3.deps_b, g64.deps_b)):
+        assert np.max(np.abs(x - y)) <= 1e-6, np.max(np.abs(x - y))
