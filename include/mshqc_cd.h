@@ -125,9 +125,10 @@ MSHQC_CD_API int mshqc_cd_cholesky_decompose(mshqc_cd_ctx* ctx, const double* er
                                              int64_t* n_vectors, int* converged, int where);
 /* Synthetic Cholesky vectors generated on the device instead of uploaded
  * (no counterpart in the reference, which takes them as data): L^Q = sigma
- * 10^(-6 Q / nvec) (X^Q + X^Q^T)/2, X^Q_{mu nu} standard normal from the
- * counter-based Philox4x32-10 generator (key = seed, counter =
- * (Q nbf + mu) nbf + nu) and Box-Muller.  The vectors are never stored: the
+ * 10^(-6 Q / nvec) (X^Q + X^Q^T)/2, X^Q standard normal: for mu <= nu one
+ * block of the counter-based Philox4x32-10 generator (key = seed, counter =
+ * (Q nbf + mu) nbf + nu) gives the Box-Muller pair (X^Q_{mu nu}, X^Q_{nu mu})
+ * (the cosine member on the diagonal).  The vectors are never stored: the
  * consumers regenerate the chunks they read, so sizes whose FP64 vectors
  * exceed device memory run (nbf = 2000, nvec = 8000: 256 GB).  The OMP2
  * entry points need stored vectors. */

@@ -291,8 +291,11 @@ class Context:
 
     def mp2_gradient_torch(self, kind: int = RESTRICTED, precision: int = FP64, device=None) -> Gradient:
         """mp2_gradient with the derivatives written straight into CUDA
-        tensors on `device` (dC as an (N, N) tensor dC[mu, p])."""
+        tensors on `device` (default: the context's GPU; dC as an (N, N)
+        tensor dC[mu, p])."""
         import torch
+        if device is None:
+            device = torch.device("cuda", self.device)
         N = self.nbf
         e = Energy()
         nspin = 2 if kind == UNRESTRICTED else 1

@@ -36,6 +36,7 @@ struct SpinState {
     DevBuf B64;
     int64_t vp = 0;
     bool B64_valid = false;
+    int B64_prec = 0;       // MSHQC_CD_FP64: FP64 products; MSHQC_CD_FP16X3: int8-slice products
     // fixed-point hi/lo (BF16 carriers) of the MO vectors for the tensor-core path
     DevBuf Bhi, Blo;
     DevBuf expo;            // per-row power-of-two exponents [o][rows]
@@ -100,6 +101,9 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf opdm;          // OMP2: OPDM blocks, densities, Fock matrices
     mshqc_cd::DevBuf omp2_ws;       // OMP2: split-K partials, rotation work matrices
     mshqc_cd::DevBuf Zt;            // OMP2: P L^Q for every Q (M*N*N)
+    mshqc_cd::DevBuf oz_a, oz_b;    // int8 slices of the transform operands (orbitals, vectors)
+    mshqc_cd::DevBuf oz_ea, oz_eb;  // their row exponents
+    mshqc_cd::DevBuf oz_flag;       // int8-slice product error flag
     bool diag_os_valid = false;
     int fixed_point_exact = 1;      // Cauchy-Schwarz bound of the last tensor-core pass held
 
@@ -118,7 +122,7 @@ struct mshqc_cd_ctx {
         for (const auto& s : spin)
             b += s.C.bytes + s.eps.bytes + s.B64.bytes + s.Bhi.bytes + s.Blo.bytes + s.expo.bytes +
                  s.diag.bytes + s.norms.bytes;
-        b += diag_os.bytes;
+        b += diag_os.bytes + oz_a.bytes + oz_b.bytes + oz_ea.bytes + oz_eb.bytes;
         for (const auto& g : gam) b += g.bytes;
         for (const auto& g : grad) b += g.bytes;
         return b;
@@ -160,6 +164,11 @@ struct mshqc_cd_ctx {
         opdm.release();
         omp2_ws.release();
         Zt.release();
+        oz_a.release();
+        oz_b.release();
+        oz_ea.release();
+        oz_eb.release();
+        oz_flag.release();
         for (auto& g : gam) g.release();
         for (auto& g : grad) g.release();
     }

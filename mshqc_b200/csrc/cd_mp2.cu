@@ -19,6 +19,7 @@
 #include "gamma_tc.cuh"
 #include "vtile_tc.cuh"
 #include "amp_elem.cuh"
+#include "ozaki_i8.cuh"
 
 namespace mshqc_cd {
 
@@ -83,6 +84,89 @@ int transform_f64(mshqc_cd_ctx* ctx, int spin) {
     CD_CUDA(gemm_f64(g2, true, true, ctx->stream));
     ctx->launches++;
     s.B64_valid = true;
+    s.B64_prec = MSHQC_CD_FP64;
+    ctx->Y_spin = spin;
+    return MSHQC_CD_OK;
+}
+
+// Bytes of int8 slices one product operand may hold (bounds the vectors
+// sub-chunks of the first product and the orbital batches of the second).
+constexpr size_t kSliceBytes = size_t(2) << 30;
+
+bool int8_transform_enabled(const mshqc_cd_ctx* ctx) {
+    if (ctx->N > ozaki::kMaxK) return false;
+    const char* env = std::getenv("MSHQC_CD_TRANSFORM");
+    return !(env && std::strcmp(env, "f64") == 0);
+}
+
+// The same half transform as transform_f64 with both products on the int8
+// tensor cores (ozaki_i8.cuh): Y = C_occ^T L per vectors chunk, then
+// B_i = C_vir^T Y_i^T in batches of occupied orbitals.  Accuracy of the
+// slices (about 2^-33 of the row maxima per term), not FP64 rounding: used by
+// the mixed-precision path only.
+int transform_i8(mshqc_cd_ctx* ctx, int spin) {
+    using namespace ozaki;
+    SpinState& s = ctx->spin[spin];
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o;
+    const int64_t vp = round_up(v, 64);
+    CD_ALLOC(ctx->Y, sizeof(double) * (size_t)o * M * N, false);
+    CD_ALLOC(s.B64, sizeof(double) * (size_t)o * vp * Mp, true);
+    CD_ALLOC(ctx->oz_flag, sizeof(int) * 2, true);
+    s.vp = vp;
+    int* err = ctx->oz_flag.as<int>();
+    const double* C = s.C.as<double>();
+    // rows of C^T: occupied orbitals (first product), virtual orbitals (second)
+    OzakiOperand Ao = ozaki_operand(o, N, BM, 1), Av = ozaki_operand(v, N, BM, 1);
+    const size_t ao_bytes = operand_bytes(Ao.Rp, Ao.Kp);
+    CD_ALLOC(ctx->oz_a, ao_bytes + operand_bytes(Av.Rp, Av.Kp), false);
+    CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(Ao.Rp + Av.Rp), false);
+    Ao.q = ctx->oz_a.as<int8_t>();  Ao.e = ctx->oz_ea.as<int>();
+    Av.q = Ao.q + ao_bytes;         Av.e = Ao.e + Ao.Rp;
+    CD_CUDA(ozaki_slice(C, N, 0, Ao, ctx->num_sms, ctx->stream));
+    CD_CUDA(ozaki_slice(C + o * N, N, 0, Av, ctx->num_sms, ctx->stream));
+    ctx->launches += 2;
+    // Y[i][(Q,nu)] = sum_mu C[mu,i] L[Q][nu*N + mu]
+    const int64_t per_q = (int64_t)operand_bytes(padded_rows(N, BN), padded_k(N));
+    const int64_t qs = std::max<int64_t>(1, (int64_t)kSliceBytes / per_q);
+    const int64_t qc = vectors_chunk_size(ctx);
+    for (int64_t Q0 = 0; Q0 < M; Q0 += qc) {
+        const int64_t mc = std::min(qc, M - Q0);
+        const double* Lc = nullptr;
+        CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
+        for (int64_t q0 = 0; q0 < mc; q0 += qs) {
+            const int64_t ms = std::min(qs, mc - q0);
+            OzakiOperand Bl = ozaki_operand(ms * N, N, BN, 1);
+            CD_ALLOC(ctx->oz_b, operand_bytes(Bl.Rp, Bl.Kp), false);
+            CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)Bl.Rp, false);
+            Bl.q = ctx->oz_b.as<int8_t>();  Bl.e = ctx->oz_eb.as<int>();
+            CD_CUDA(ozaki_slice(Lc + q0 * N * N, N, 0, Bl, ctx->num_sms, ctx->stream));
+            CD_CUDA(ozaki_gemm(Ao, true, Bl, ctx->Y.as<double>() + (Q0 + q0) * N, M * N, 0, 1.0, 0.0, err,
+                               ctx->num_sms, ctx->stream));
+            ctx->launches += 2;
+        }
+    }
+    // B[i][a][Q] = sum_nu C[nu, o+a] Y[i][Q][nu], a batch of orbitals i at a time
+    const int64_t per_i = (int64_t)operand_bytes(padded_rows(M, BN), padded_k(N));
+    const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)kSliceBytes / per_i));
+    for (int64_t i0 = 0; i0 < o; i0 += ib) {
+        const int64_t nb = std::min(ib, o - i0);
+        OzakiOperand By = ozaki_operand(M, N, BN, (int)nb);
+        CD_ALLOC(ctx->oz_b, operand_bytes(By.Rp, By.Kp) * (size_t)nb, false);
+        CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(By.Rp * nb), false);
+        By.q = ctx->oz_b.as<int8_t>();  By.e = ctx->oz_eb.as<int>();
+        CD_CUDA(ozaki_slice(ctx->Y.as<double>() + i0 * M * N, N, M * N, By, ctx->num_sms, ctx->stream));
+        CD_CUDA(ozaki_gemm(Av, true, By, s.B64.as<double>() + i0 * vp * Mp, Mp, vp * Mp, 1.0, 0.0, err,
+                           ctx->num_sms, ctx->stream));
+        ctx->launches += 2;
+    }
+    int herr = 0;
+    CD_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (herr)
+        return set_error(MSHQC_CD_ERR_TIMEOUT, "int8 tensor-core transform gave up waiting (site " +
+                                                   std::to_string(herr) + ")");
+    s.B64_valid = true;
+    s.B64_prec = MSHQC_CD_FP16X3;
     ctx->Y_spin = spin;
     return MSHQC_CD_OK;
 }
@@ -418,9 +502,13 @@ int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
     SpinState& s = ctx->spin[spin];
     if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_FP16X3)
         return set_error(MSHQC_CD_ERR_ARG, "unknown precision");
-    if (!s.B64_valid) {
+    // an FP64 request never reuses int8-slice products; a mixed one reuses either
+    if (!s.B64_valid || (precision == MSHQC_CD_FP64 && s.B64_prec != MSHQC_CD_FP64)) {
         begin_stage(ctx, ST_TRANSFORM);
-        CD_RC(transform_f64(ctx, spin));
+        if (precision == MSHQC_CD_FP16X3 && int8_transform_enabled(ctx))
+            CD_RC(transform_i8(ctx, spin));
+        else
+            CD_RC(transform_f64(ctx, spin));
         end_stage(ctx);
         s.B16_valid = false;
     }
@@ -741,7 +829,10 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
     const int64_t Mp = ctx->Mp;
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t budget = std::min<size_t>(free_b / 3, size_t(40) << 30);
+    // the staging this pass reuses counts as available, so that the block size
+    // of a repeated call does not shrink because the previous call holds it
+    const size_t held = ctx->amp.bytes + ctx->amp2.bytes + ctx->ampT.bytes + ctx->ampT2.bytes + ctx->W.bytes;
+    const size_t budget = std::min<size_t>((free_b + held) / 3, size_t(40) << 30);
     // block sizes: rows bI, columns bJ (all of them for the opposite spin)
     int64_t bI, bJ;
     if (kSym) {

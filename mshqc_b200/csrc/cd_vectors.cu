@@ -7,11 +7,14 @@
 // forward half transform, the dE/dC_occ transposed transform) asks for
 // chunks of Q and they are generated again each time.
 //
-// X^Q_{mu nu} = Box-Muller normal of one Philox4x32-10 block (the counter-based
-// generator of Salmon, Moraes, Dror and Shaw, SC 2011) with key = seed and
-// counter = (Q N + mu) N + nu: u1 from the first 64 output bits, u2 from the
-// second, z = sqrt(-2 ln u1) cos(2 pi u2).  mshqc_b200/synthetic.py holds the
-// same recipe in numpy (make_vectors_philox) for the tests.
+// For mu < nu one Philox4x32-10 block (the counter-based generator of Salmon,
+// Moraes, Dror and Shaw, SC 2011) with key = seed and counter
+// (Q N + mu) N + nu gives u1 (first 64 output bits) and u2 (second) and the
+// Box-Muller pair r = sqrt(-2 ln u1), X^Q_{mu nu} = r cos(2 pi u2),
+// X^Q_{nu mu} = r sin(2 pi u2): two independent N(0, 1) draws, so one
+// logarithm and one sincos per symmetric element pair.  X^Q_{mu mu} is the
+// cosine member of counter (Q N + mu) N + mu.  mshqc_b200/synthetic.py holds
+// the same recipe in numpy (make_vectors_philox) for the tests.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,13 +47,18 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32
     }
 }
 
-__device__ __forceinline__ double std_normal(uint64_t seed, uint64_t ctr) {
+// Box-Muller pair (r cos 2 pi u2, r sin 2 pi u2) of one Philox block
+__device__ __forceinline__ void std_normal_pair(uint64_t seed, uint64_t ctr, double* zc, double* zs) {
     uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u};
     philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
     const uint64_t a = ((uint64_t)c[0] << 32) | c[1], b = ((uint64_t)c[2] << 32) | c[3];
     const double u1 = ((double)(a >> 11) + 0.5) * 0x1.0p-53;
     const double u2 = ((double)(b >> 11) + 0.5) * 0x1.0p-53;
-    return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    const double r = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    *zc = r * cs;
+    *zs = r * sn;
 }
 
 // One 32 x 32 tile pair (row block x <= column block y) of vector Q0 + q:
@@ -71,8 +79,11 @@ __global__ void __launch_bounds__(256) gen_vectors_kernel(uint64_t seed, const d
         const int64_t mu = (int64_t)x * 32 + r, nu = (int64_t)y * 32 + tx;
         double v = 0.0;
         if (mu < N && nu < N) {
-            const double z1 = std_normal(seed, ((uint64_t)Q * N + mu) * N + nu);
-            const double z2 = std_normal(seed, ((uint64_t)Q * N + nu) * N + mu);
+            // the pair's block sits at counter (Q N + min) N + max (x < y: mu < nu)
+            const int64_t lo = mu < nu ? mu : nu, hi = mu < nu ? nu : mu;
+            double z1, z2;
+            std_normal_pair(seed, ((uint64_t)Q * N + lo) * N + hi, &z1, &z2);
+            if (mu == nu) z2 = z1;
             v = s * (0.5 * (z1 + z2));
             o[mu * N + nu] = v;
         }

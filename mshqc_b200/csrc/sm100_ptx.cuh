@@ -107,6 +107,15 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
+// D[tmem] (+)= A * B^T, signed 8-bit integers, exact 32-bit integer accumulation
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
 // Arrive on bar once all previously issued tcgen05 ops of this thread completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile(
@@ -152,6 +161,15 @@ __device__ __forceinline__ void tmem_ld_wait() {
 // Instruction descriptor, kind::f16: FP16 x FP16 -> FP32, both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
     return (1u << 4)                        // D format: F32; A, B format 0: F16
+           | ((uint32_t)(N >> 3) << 17)     // N / 8
+           | ((uint32_t)(M >> 4) << 24);    // M / 16
+}
+
+// Instruction descriptor, kind::i8: S8 x S8 -> S32, both operands K-major.
+__host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
+    return (2u << 4)                        // D format: S32
+           | (1u << 7)                      // A format: signed 8-bit
+           | (1u << 10)                     // B format: signed 8-bit
            | ((uint32_t)(N >> 3) << 17)     // N / 8
            | ((uint32_t)(M >> 4) << 24);    // M / 16
 }

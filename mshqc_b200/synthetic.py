@@ -206,19 +206,29 @@ def philox4x32_10_words(c0, c1, c2, c3, key0: int, key1: int) -> tuple:
     return c0, c1, c2, c3
 
 
-def philox_normal(ctr: np.ndarray, seed: int) -> np.ndarray:
-    """Box-Muller standard normal of one Philox block per counter."""
+def philox_normal_pair(ctr: np.ndarray, seed: int) -> tuple:
+    """Box-Muller pair of independent standard normals from one Philox block
+    per counter: r = sqrt(-2 ln u1), (r cos 2 pi u2, r sin 2 pi u2), with u1
+    from the first 64 output bits and u2 from the second."""
     c0, c1, c2, c3 = philox4x32_10(ctr, seed)
     a = (c0.astype(np.uint64) << np.uint64(32)) | c1.astype(np.uint64)
     b = (c2.astype(np.uint64) << np.uint64(32)) | c3.astype(np.uint64)
     u1 = ((a >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
     u2 = ((b >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
-    return np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586 * u2)
+    r = np.sqrt(-2.0 * np.log(u1))
+    return r * np.cos(6.283185307179586 * u2), r * np.sin(6.283185307179586 * u2)
+
+
+def philox_normal(ctr: np.ndarray, seed: int) -> np.ndarray:
+    """The first (cosine) member of philox_normal_pair."""
+    return philox_normal_pair(ctr, seed)[0]
 
 
 def make_vectors_philox(N: int, M: int, seed: int, sigma: float = 1.0) -> np.ndarray:
     """The recipe as the library's device generator draws it
-    (mshqc_cd_gen_vectors): X^Q_{mu nu} = philox_normal((Q N + mu) N + nu),
+    (mshqc_cd_gen_vectors): for mu < nu one Philox block with counter
+    (Q N + mu) N + nu gives the Box-Muller pair (X^Q_{mu nu}, X^Q_{nu mu}), the
+    diagonal X^Q_{mu mu} is the cosine member of counter (Q N + mu) N + mu, and
     L^Q = sigma 10^(-6Q/M) (X + X^T)/2.  (M, N*N) float64; for small sizes."""
     s = scale_factors(M) * sigma
     L = np.empty((M, N * N), dtype=np.float64)
@@ -226,8 +236,9 @@ def make_vectors_philox(N: int, M: int, seed: int, sigma: float = 1.0) -> np.nda
     nu = np.arange(N, dtype=np.uint64)[None, :]
     for q in range(M):
         base = np.uint64(q) * np.uint64(N)
-        Z = philox_normal((base + mu) * np.uint64(N) + nu, seed)
-        L[q] = (s[q] * (0.5 * (Z + Z.T))).reshape(N * N)
+        Zc, Zs = philox_normal_pair((base + mu) * np.uint64(N) + nu, seed)
+        X = np.triu(Zc, 1) + np.triu(Zs, 1).T + np.diag(np.diag(Zc))
+        L[q] = (s[q] * (0.5 * (X + X.T))).reshape(N * N)
     return L
 
 

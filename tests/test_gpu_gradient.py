@@ -70,10 +70,24 @@ def test_restricted_mixed_gradient_vs_fp64(ctx, N, o, M, seed):
     a = inp.alpha
     ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
     g64 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
+    ctx.set_orbitals(capi.ALPHA, a.C, a.eps, o)      # mixed transform (int8 slices), not the FP64 one
     g3 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
     assert abs(g3.energy["total"] - g64.energy["total"]) <= 1e-6
     assert np.max(np.abs(g3.dC_a - g64.dC_a)) <= 1e-6, np.max(np.abs(g3.dC_a - g64.dC_a))
     assert np.max(np.abs(g3.deps_a - g64.deps_a)) <= 1e-6, np.max(np.abs(g3.deps_a - g64.deps_a))
+
+
+def test_gradient_torch_defaults_to_context_gpu(ctx):
+    import torch
+    inp = twin(40, 5, 90, seed=12)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, 5)
+    g = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
+    gt = ctx.mp2_gradient_torch(capi.RESTRICTED, capi.FP64)
+    assert gt.dC_a.is_cuda and gt.dC_a.device.index == ctx.device
+    assert np.array_equal(gt.dC_a.cpu().numpy(), g.dC_a)
+    # dE/deps sums per-block partials in launch order: equal to rounding
+    assert np.allclose(gt.deps_a.cpu().numpy(), g.deps_a, rtol=1e-12, atol=1e-15)
 
 
 def test_restricted_mixed_gradient_vs_oracle(ctx):
@@ -173,6 +187,7 @@ def test_unrestricted_mixed_gradient_vs_fp64(ctx, N, oa, ob, M, seed):
     inp = twin(N, oa, M, seed=seed, nocc_beta=ob)
     set_unrestricted(ctx, inp)
     g64 = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP64)
+    set_unrestricted(ctx, inp)                        # mixed transforms of both spins
     g3 = ctx.mp2_gradient(capi.UNRESTRICTED, capi.FP16X3)
     for key in ("ss_aa", "ss_bb", "os", "total"):
         assert abs(g3.energy[key] - g64.energy[key]) <= 1e-6, key

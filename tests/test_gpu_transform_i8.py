@@ -1,0 +1,95 @@
+"""Half transform of the mixed path on the int8 tensor cores (ozaki_i8.cuh:
+every operand row cut into five 7-bit slices under a per-row power of two,
+exact int32 products, FP64 combination) against the CPU oracle and the FP64
+path.
+
+The slice products carry an error of about 2^-31 of (row max x row max) per
+term, so the transformed vectors agree with the FP64 ones to
+REL_TOL = 2e-8 of max |B| (the FP64 path: 1e-13).  An FP64 request after a
+mixed one recomputes the vectors in FP64; MSHQC_CD_TRANSFORM=f64 sends the
+mixed path through the FP64 transform.
+"""
+import numpy as np
+import pytest
+
+from mshqc_b200 import capi
+from mshqc_b200 import synthetic as syn
+from oracle import cdmp2_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 2e-8
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+def rel_err(B, Bref):
+    return np.max(np.abs(B - Bref)) / np.max(np.abs(Bref))
+
+
+@pytest.mark.parametrize("name", ["rmp2_ragged_n29_o7_m61", "rmp2_n32_o6_m96", "rmp2_single_occupied"])
+def test_mixed_transform_vs_oracle(ctx, golden, name):
+    g = golden(name)
+    o = int(g["nocc"])
+    ctx.set_vectors(g["L"]).set_orbitals(capi.ALPHA, g["C"], g["eps"], o)
+    B = ctx.transform(capi.ALPHA, capi.FP16X3)
+    Bref = orc.transform(g["L"], g["C"], o)
+    assert B.shape == Bref.shape
+    assert rel_err(B, Bref) <= REL_TOL
+    # an FP64 request does not reuse the int8-slice vectors
+    B64 = ctx.transform(capi.ALPHA, capi.FP64)
+    assert np.max(np.abs(B64 - Bref)) <= 1e-13 * np.max(np.abs(Bref))
+
+
+@pytest.mark.parametrize("N,o,M", [(257, 19, 515), (300, 30, 1200), (161, 1, 97), (96, 95, 33)])
+def test_mixed_transform_vs_fp64(ctx, N, o, M):
+    inp = syn.make_inputs(N, o, M, seed=N + o)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    B64 = ctx.transform(capi.ALPHA, capi.FP64)
+    ctx.set_orbitals(capi.ALPHA, a.C, a.eps, o)    # drop the FP64 vectors
+    B8 = ctx.transform(capi.ALPHA, capi.FP16X3)
+    assert rel_err(B8, B64) <= REL_TOL, rel_err(B8, B64)
+
+
+def test_env_switch_selects_fp64_transform(ctx, monkeypatch):
+    inp = syn.make_inputs(120, 12, 300, seed=5)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, 12)
+    B64 = ctx.transform(capi.ALPHA, capi.FP64)
+    monkeypatch.setenv("MSHQC_CD_TRANSFORM", "f64")
+    ctx.set_orbitals(capi.ALPHA, a.C, a.eps, 12)
+    B = ctx.transform(capi.ALPHA, capi.FP16X3)
+    assert np.array_equal(B, B64)
+
+
+@pytest.mark.parametrize("chunk", [None, "7"])
+def test_generated_vectors_mixed_transform(monkeypatch, chunk):
+    N, o, M, seed = 70, 9, 130, 11
+    if chunk:
+        monkeypatch.setenv("MSHQC_CD_GEN_CHUNK", chunk)
+    orb = syn.make_orbitals(N, o, 3)
+    L = syn.make_vectors_philox(N, M, seed, 0.01)
+    with capi.Context(0) as c:
+        c.gen_vectors(N, M, seed, 0.01)
+        c.set_orbitals(capi.ALPHA, orb.C, orb.eps, o)
+        B = c.transform(capi.ALPHA, capi.FP16X3)
+    Bref = orc.transform(L, orb.C, o)
+    assert rel_err(B, Bref) <= REL_TOL
+
+
+def test_mixed_energy_with_int8_transform_vs_fp64(ctx):
+    N, o, M = 200, 20, 800
+    base = syn.make_inputs(N, o, M, seed=9)
+    sig = syn.twin_sigma(N, o, M, base.alpha.eps)
+    inp = syn.make_inputs(N, o, M, seed=9, sigma=sig)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    e3 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
+    e64 = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)
+    assert abs(e3["total"] - e64["total"]) <= 1e-6

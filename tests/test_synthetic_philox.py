@@ -32,10 +32,16 @@ def test_counter_form_matches_words():
 
 
 def test_normals_and_vectors():
-    z = syn.philox_normal(np.arange(400000, dtype=np.uint64), 9)
-    assert abs(z.mean()) < 0.01 and abs(z.var() - 1.0) < 0.01 and abs(np.mean(z ** 4) - 3.0) < 0.05
+    zc, zs = syn.philox_normal_pair(np.arange(400000, dtype=np.uint64), 9)
+    for z in (zc, zs):
+        assert abs(z.mean()) < 0.01 and abs(z.var() - 1.0) < 0.01 and abs(np.mean(z ** 4) - 3.0) < 0.05
+    assert abs(np.mean(zc * zs)) < 0.01          # the two members are uncorrelated
     L = syn.make_vectors_philox(9, 5, seed=3, sigma=0.5).reshape(5, 9, 9)
     assert np.array_equal(L, L.transpose(0, 2, 1))
-    # diagonal element = sigma s_Q X_{mu mu}
+    sq = syn.scale_factors(5)[2] * 0.5
+    # diagonal element = sigma s_Q X_{mu mu} (cosine member)
     x = syn.philox_normal(np.array([(2 * 9 + 4) * 9 + 4], dtype=np.uint64), 3)[0]
-    assert L[2, 4, 4] == syn.scale_factors(5)[2] * 0.5 * x
+    assert L[2, 4, 4] == sq * (0.5 * (x + x))
+    # off-diagonal (mu < nu): both members of the block at counter (Q N + mu) N + nu
+    c, s = syn.philox_normal_pair(np.array([(2 * 9 + 1) * 9 + 6], dtype=np.uint64), 3)
+    assert L[2, 1, 6] == L[2, 6, 1] == sq * (0.5 * (c[0] + s[0]))
