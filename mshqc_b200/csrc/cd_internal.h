@@ -104,6 +104,7 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf oz_a, oz_b;    // int8 slices of the transform operands (orbitals, vectors)
     mshqc_cd::DevBuf oz_ea, oz_eb;  // their row exponents
     mshqc_cd::DevBuf oz_flag;       // int8-slice product error flag
+    mshqc_cd::DevBuf oz_p;          // per-batch FP64 partial products (transposed transforms)
     bool diag_os_valid = false;
     int fixed_point_exact = 1;      // Cauchy-Schwarz bound of the last tensor-core pass held
 
@@ -122,7 +123,7 @@ struct mshqc_cd_ctx {
         for (const auto& s : spin)
             b += s.C.bytes + s.eps.bytes + s.B64.bytes + s.Bhi.bytes + s.Blo.bytes + s.expo.bytes +
                  s.diag.bytes + s.norms.bytes;
-        b += diag_os.bytes + oz_a.bytes + oz_b.bytes + oz_ea.bytes + oz_eb.bytes;
+        b += diag_os.bytes + oz_a.bytes + oz_b.bytes + oz_ea.bytes + oz_eb.bytes + oz_p.bytes;
         for (const auto& g : gam) b += g.bytes;
         for (const auto& g : grad) b += g.bytes;
         return b;
@@ -169,6 +170,7 @@ struct mshqc_cd_ctx {
         oz_ea.release();
         oz_eb.release();
         oz_flag.release();
+        oz_p.release();
         for (auto& g : gam) g.release();
         for (auto& g : grad) g.release();
     }

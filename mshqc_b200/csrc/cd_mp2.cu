@@ -140,7 +140,7 @@ int transform_i8(mshqc_cd_ctx* ctx, int spin) {
             CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)Bl.Rp, false);
             Bl.q = ctx->oz_b.as<int8_t>();  Bl.e = ctx->oz_eb.as<int>();
             CD_CUDA(ozaki_slice(Lc + q0 * N * N, N, 0, Bl, ctx->num_sms, ctx->stream));
-            CD_CUDA(ozaki_gemm(Ao, true, Bl, ctx->Y.as<double>() + (Q0 + q0) * N, M * N, 0, 1.0, 0.0, err,
+            CD_CUDA(ozaki_gemm(Ao, true, Bl, false, ctx->Y.as<double>() + (Q0 + q0) * N, M * N, 0, 1.0, 0.0, err,
                                ctx->num_sms, ctx->stream));
             ctx->launches += 2;
         }
@@ -155,7 +155,7 @@ int transform_i8(mshqc_cd_ctx* ctx, int spin) {
         CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(By.Rp * nb), false);
         By.q = ctx->oz_b.as<int8_t>();  By.e = ctx->oz_eb.as<int>();
         CD_CUDA(ozaki_slice(ctx->Y.as<double>() + i0 * M * N, N, M * N, By, ctx->num_sms, ctx->stream));
-        CD_CUDA(ozaki_gemm(Av, true, By, s.B64.as<double>() + i0 * vp * Mp, Mp, vp * Mp, 1.0, 0.0, err,
+        CD_CUDA(ozaki_gemm(Av, true, By, false, s.B64.as<double>() + i0 * vp * Mp, Mp, vp * Mp, 1.0, 0.0, err,
                            ctx->num_sms, ctx->stream));
         ctx->launches += 2;
     }
@@ -660,6 +660,141 @@ int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC)
     return MSHQC_CD_OK;
 }
 
+// out[k] = (accumulate ? out[k] : 0) + alpha * sum_b parts[b * n + k], b in order
+__global__ void sum_batches_kernel(const double* __restrict__ parts, int nb, int64_t n, double alpha,
+                                   int accumulate, double* __restrict__ out) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double acc = 0.0;
+    for (int b = 0; b < nb; ++b) acc += parts[(int64_t)b * n + k];
+    out[k] = accumulate ? out[k] + alpha * acc : alpha * acc;
+}
+
+int sum_batches(mshqc_cd_ctx* ctx, const double* parts, int nb, int64_t n, double alpha, bool accumulate,
+                double* out) {
+    sum_batches_kernel<<<(unsigned)cdiv(n, 256), 256, 0, ctx->stream>>>(parts, nb, n, alpha, accumulate ? 1 : 0,
+                                                                         out);
+    CD_CUDA(cudaGetLastError());
+    ctx->launches++;
+    return MSHQC_CD_OK;
+}
+
+// The transposed transforms of the mixed path on the int8 tensor cores
+// (ozaki_i8.cuh), batched so that every product has K = M, v or N:
+//   dC[nu, o+a] = scale sum_i (Gamma_i Y_i)[a][nu]        batches of i, partials summed in order
+//   W_i[Q][nu]  = sum_a Gamma_i[a][Q] C[nu, o+a]           batches of i, C_vir shared
+//   dC[mu, i]   = scale sum_Q (W_Q L_Q)[i][mu]             batches of Q per vectors chunk
+// with W_Q[i][nu] = W[i][Q][nu] and L_Q[mu][nu] = L[Q][nu][mu].
+int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* dC) {
+    using namespace ozaki;
+    SpinState& s = ctx->spin[spin];
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o;
+    if (ctx->Y_spin != spin) {
+        s.B64_valid = false;
+        CD_RC(transform_i8(ctx, spin));
+    }
+    const int64_t vp = s.vp;
+    const double* C = s.C.as<double>();
+    const double* Gm = ctx->gam[spin].as<double>();
+    double* Y = ctx->Y.as<double>();
+    CD_ALLOC(ctx->oz_flag, sizeof(int) * 2, true);
+    int* err = ctx->oz_flag.as<int>();
+    // dC[nu, o+a]: A = Gamma_i (rows a, K = Q), B = Y_i^T (rows nu, K = Q, strided by N)
+    {
+        const size_t pa = operand_bytes(padded_rows(v, BM), padded_k(M));
+        const size_t pb = operand_bytes(padded_rows(N, BN), padded_k(M));
+        const size_t pp = sizeof(double) * (size_t)(v * N);
+        const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(2 * kSliceBytes / (pa + pb + pp))));
+        CD_ALLOC(ctx->oz_a, pa * ib, false);
+        CD_ALLOC(ctx->oz_b, pb * ib, false);
+        CD_ALLOC(ctx->oz_p, pp * ib, false);
+        CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(v, BM) * ib), false);
+        CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(padded_rows(N, BN) * ib), false);
+        for (int64_t i0 = 0; i0 < o; i0 += ib) {
+            const int64_t nb = std::min(ib, o - i0);
+            OzakiOperand A = ozaki_operand(v, M, BM, (int)nb), B = ozaki_operand(N, M, BN, (int)nb);
+            A.q = ctx->oz_a.as<int8_t>();  A.e = ctx->oz_ea.as<int>();
+            B.q = ctx->oz_b.as<int8_t>();  B.e = ctx->oz_eb.as<int>();
+            CD_CUDA(ozaki_slice(Gm + i0 * vp * Mp, Mp, vp * Mp, A, ctx->num_sms, ctx->stream));
+            CD_CUDA(ozaki_slice_t(Y + i0 * M * N, N, M * N, B, ctx->stream));
+            CD_CUDA(ozaki_gemm(A, false, B, false, ctx->oz_p.as<double>(), N, v * N, 1.0, 0.0, err, ctx->num_sms,
+                               ctx->stream));
+            ctx->launches += 5;
+            CD_RC(sum_batches(ctx, ctx->oz_p.as<double>(), (int)nb, v * N, scale, i0 > 0, dC + o * N));
+        }
+    }
+    // W[i][Q][nu] into the Y buffer: A = Gamma_i^T (rows Q, K = a, strided by Mp),
+    // B = C_vir^T (rows nu, K = a, strided by N), shared
+    {
+        OzakiOperand B = ozaki_operand(N, v, BN, 1);
+        const size_t pa = operand_bytes(padded_rows(M, BM), padded_k(v));
+        const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(kSliceBytes / pa)));
+        CD_ALLOC(ctx->oz_a, pa * ib, false);
+        CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(M, BM) * ib), false);
+        CD_ALLOC(ctx->oz_b, operand_bytes(B.Rp, B.Kp), false);
+        CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)B.Rp, false);
+        B.q = ctx->oz_b.as<int8_t>();  B.e = ctx->oz_eb.as<int>();
+        CD_CUDA(ozaki_slice_t(C + o * N, N, 0, B, ctx->stream));
+        ctx->launches += 3;
+        for (int64_t i0 = 0; i0 < o; i0 += ib) {
+            const int64_t nb = std::min(ib, o - i0);
+            OzakiOperand A = ozaki_operand(M, v, BM, (int)nb);
+            A.q = ctx->oz_a.as<int8_t>();  A.e = ctx->oz_ea.as<int>();
+            CD_CUDA(ozaki_slice_t(Gm + i0 * vp * Mp, Mp, vp * Mp, A, ctx->stream));
+            CD_CUDA(ozaki_gemm(A, false, B, true, Y + i0 * M * N, N, M * N, 1.0, 0.0, err, ctx->num_sms,
+                               ctx->stream));
+            ctx->launches += 4;
+        }
+        ctx->Y_spin = -1;
+    }
+    // dC[mu, i]: A = W_Q (rows i, K = nu), B = L_Q (rows mu, K = nu, strided by N)
+    {
+        const size_t pa = operand_bytes(padded_rows(o, BM), padded_k(N));
+        const size_t pb = operand_bytes(padded_rows(N, BN), padded_k(N));
+        const size_t pp = sizeof(double) * (size_t)(o * N);
+        const int64_t nq_max = std::max<int64_t>(1, (int64_t)(2 * kSliceBytes / (pa + pb + pp)));
+        const int64_t qc = vectors_chunk_size(ctx);
+        const int64_t nq = std::min(nq_max, qc);
+        CD_ALLOC(ctx->oz_a, pa * nq, false);
+        CD_ALLOC(ctx->oz_b, pb * nq, false);
+        CD_ALLOC(ctx->oz_p, pp * nq, false);
+        CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(o, BM) * nq), false);
+        CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(padded_rows(N, BN) * nq), false);
+        for (int64_t Q0 = 0; Q0 < M; Q0 += qc) {
+            const int64_t mc = std::min(qc, M - Q0);
+            const double* Lc = nullptr;
+            CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
+            for (int64_t q0 = 0; q0 < mc; q0 += nq) {
+                const int64_t nb = std::min(nq, mc - q0);
+                OzakiOperand A = ozaki_operand(o, N, BM, (int)nb), B = ozaki_operand(N, N, BN, (int)nb);
+                A.q = ctx->oz_a.as<int8_t>();  A.e = ctx->oz_ea.as<int>();
+                B.q = ctx->oz_b.as<int8_t>();  B.e = ctx->oz_eb.as<int>();
+                CD_CUDA(ozaki_slice(Y + (Q0 + q0) * N, M * N, N, A, ctx->num_sms, ctx->stream));
+                CD_CUDA(ozaki_slice_t(Lc + q0 * N * N, N, N * N, B, ctx->stream));
+                CD_CUDA(ozaki_gemm(A, false, B, false, ctx->oz_p.as<double>(), N, o * N, 1.0, 0.0, err,
+                                   ctx->num_sms, ctx->stream));
+                ctx->launches += 5;
+                CD_RC(sum_batches(ctx, ctx->oz_p.as<double>(), (int)nb, o * N, scale, Q0 + q0 > 0, dC));
+            }
+        }
+    }
+    int herr = 0;
+    CD_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (herr)
+        return set_error(MSHQC_CD_ERR_TIMEOUT, "int8 tensor-core transposed transform gave up waiting (site " +
+                                                   std::to_string(herr) + ")");
+    return MSHQC_CD_OK;
+}
+
+// dE/dC of one spin: the int8-slice transposed transforms for the mixed path
+// (unless switched off), FP64 otherwise
+int transposed_dispatch(mshqc_cd_ctx* ctx, int spin, double scale, double* dC, int precision) {
+    if (precision == MSHQC_CD_FP16X3 && int8_transform_enabled(ctx))
+        return transposed_transforms_i8(ctx, spin, scale, dC);
+    return transposed_transforms(ctx, spin, scale, dC);
+}
+
 // Restricted FP64 gradient: amplitude pass + Gamma GEMM per block of occupied
 // rows, then the transposed half transforms.  dC (column-major N*N, device),
 // deps (N, device) are written; *energy gets the closed-shell E.
@@ -1032,7 +1167,7 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
                                                    std::to_string(herr[0] ? herr[0] : herr[2]) + ")");
     if (herr[1]) ctx->fixed_point_exact = 0;
     begin_stage(ctx, ST_TRANSPOSED);
-    CD_RC(transposed_transforms(ctx, 0, 4.0, dC));
+    CD_RC(transposed_dispatch(ctx, 0, 4.0, dC, MSHQC_CD_FP16X3));
     end_stage(ctx);
     return MSHQC_CD_OK;
 }
@@ -1084,8 +1219,8 @@ int gradient_unrestricted(mshqc_cd_ctx* ctx, int precision, double* const dC[2],
                                                    std::to_string(herr[0] ? herr[0] : herr[2]) + ")");
     if (herr[1]) ctx->fixed_point_exact = 0;
     begin_stage(ctx, ST_TRANSPOSED);
-    CD_RC(transposed_transforms(ctx, 0, 2.0, dC[0]));
-    CD_RC(transposed_transforms(ctx, 1, 2.0, dC[1]));
+    CD_RC(transposed_dispatch(ctx, 0, 2.0, dC[0], precision));
+    CD_RC(transposed_dispatch(ctx, 1, 2.0, dC[1], precision));
     end_stage(ctx);
     return MSHQC_CD_OK;
 }

@@ -132,6 +132,84 @@ static __global__ void ozaki_slice_kernel(const double* __restrict__ src, long l
     }
 }
 
+// Slices of the rows of matrices stored with the rows contiguous and K
+// strided (batch b: element (r, k) at src + b * src_batch + k * ld + r), in
+// three passes: row maxima over K splits (atomicMax of the frexp exponent
+// into e, which starts at kNoExponent), exponents of empty or tiny rows set
+// to 0, then one thread per (row, 16-wide K group) writing the S digits.
+namespace ozaki {
+constexpr int kNoExponent = (int)0x80808080;   // byte pattern 0x80 (memset)
+constexpr int kTinyExponent = -890;            // rows below 2^-890 are sliced as zero
+constexpr int kRowmaxSpan = 512;               // K elements per row-maximum thread
+}  // namespace ozaki
+
+static __global__ void __launch_bounds__(256) ozaki_rowmax_t_kernel(const double* __restrict__ src, long long ld,
+                                                                    long long src_batch, long long R, long long K,
+                                                                    long long Rp, int* __restrict__ e) {
+    using namespace ozaki;
+    const long long r = blockIdx.x * 256LL + threadIdx.x;
+    const long long b = blockIdx.z;
+    if (r >= R) return;
+    const long long k0 = (long long)blockIdx.y * kRowmaxSpan, k1 = std::min<long long>(K, k0 + kRowmaxSpan);
+    const double* col = src + b * src_batch + r;
+    double mx = 0.0;
+    for (long long k = k0; k < k1; ++k) mx = fmax(mx, fabs(col[k * ld]));
+    if (mx > 0.0) {
+        int ex = 0;
+        frexp(mx, &ex);
+        atomicMax(e + b * Rp + r, ex);
+    }
+}
+
+static __global__ void ozaki_exp_fix_kernel(int* __restrict__ e, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n && e[i] < ozaki::kTinyExponent) e[i] = 0;
+}
+
+// grid (Rp / 32, ceil(Kp / 128), batch), 256 threads: lane -> row, warp -> 16-wide K group
+static __global__ void __launch_bounds__(256) ozaki_slice_t_kernel(const double* __restrict__ src, long long ld,
+                                                                   long long src_batch, long long R, long long K,
+                                                                   long long Rp, long long Kp,
+                                                                   const int* __restrict__ e,
+                                                                   int8_t* __restrict__ dst) {
+    using namespace ozaki;
+    const int lane = threadIdx.x & 31;
+    const long long r = blockIdx.x * 32LL + lane;
+    const long long k0 = ((long long)blockIdx.y * 8 + (threadIdx.x >> 5)) * 16;
+    const long long b = blockIdx.z;
+    if (k0 >= Kp) return;
+    const bool live = r < R;
+    const int ex = e[b * Rp + r];
+    const double to_fixed = pow2d(7 * S - ex);
+    constexpr long long kMaxFixed = (1LL << (7 * S)) - 1;
+    const double* col = src + b * src_batch + r;
+    uint32_t word[S][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) word[s][q] = 0u;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const long long k = k0 + q * 4 + c;
+            const double xs = (live && k < K) ? col[k * ld] * to_fixed : 0.0;
+            const long long m = __double2ll_rn(xs);
+            const bool neg = m < 0;
+            const unsigned long long am = (unsigned long long)min(neg ? -m : m, kMaxFixed);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t d = (uint32_t)(am >> (7 * (S - 1 - s))) & 127u;
+                word[s][q] |= ((neg ? 0u - d : d) & 0xFFu) << (8 * c);
+            }
+        }
+    }
+    int8_t* out = dst + b * (long long)S * Kp * Rp + (k0 >> 5) * Rp * KB +
+                  (((r >> 3) * 2 + ((k0 & 31) >> 4)) << 7) + ((r & 7) << 4);
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        *reinterpret_cast<uint4*>(out + (long long)s * Kp * Rp) =
+            make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
+}
+
 struct OzakiArgs {
     const int8_t* A; long long a_batch; long long RpA; const int* eA; long long ea_batch;
     const int8_t* B; long long b_batch; long long RpB; const int* eB; long long eb_batch;
@@ -370,9 +448,32 @@ inline cudaError_t ozaki_slice(const double* src, long long ld, long long src_ba
     return cudaGetLastError();
 }
 
-// C[b] = alpha * A[b or 0] B[b]^T + beta * C[b]; a_shared: one A for all batches.
-inline cudaError_t ozaki_gemm(const OzakiOperand& A, bool a_shared, const OzakiOperand& B, double* C,
-                              long long ldc, long long c_batch, double alpha, double beta, int* err,
+// Transposed source: element (r, k) of batch b at src + b * src_batch + k * ld + r.
+inline cudaError_t ozaki_slice_t(const double* src, long long ld, long long src_batch, const OzakiOperand& op,
+                                 cudaStream_t st) {
+    using namespace ozaki;
+    cudaError_t err = cudaMemsetAsync(op.e, 0x80, sizeof(int) * (size_t)(op.Rp * op.batch), st);
+    if (err != cudaSuccess) return err;
+    if (op.R > 0 && op.K > 0) {
+        dim3 g1((unsigned)((op.R + 255) / 256), (unsigned)((op.K + kRowmaxSpan - 1) / kRowmaxSpan),
+                (unsigned)op.batch);
+        ozaki_rowmax_t_kernel<<<g1, 256, 0, st>>>(src, ld, src_batch, op.R, op.K, op.Rp, op.e);
+        err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+    }
+    const long long n = op.Rp * op.batch;
+    ozaki_exp_fix_kernel<<<(unsigned)std::max<long long>(1, (n + 255) / 256), 256, 0, st>>>(op.e, n);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    dim3 g2((unsigned)(op.Rp / 32), (unsigned)((op.Kp + 127) / 128), (unsigned)op.batch);
+    ozaki_slice_t_kernel<<<g2, 256, 0, st>>>(src, ld, src_batch, op.R, op.K, op.Rp, op.Kp, op.e, op.q);
+    return cudaGetLastError();
+}
+
+// C[b] = alpha * A[b] B[b]^T + beta * C[b] over the batches; a shared operand
+// (a_shared / b_shared) is one matrix used by every batch.
+inline cudaError_t ozaki_gemm(const OzakiOperand& A, bool a_shared, const OzakiOperand& B, bool b_shared,
+                              double* C, long long ldc, long long c_batch, double alpha, double beta, int* err,
                               int num_sms, cudaStream_t st) {
     using namespace ozaki;
     static bool attr_set[64] = {};
@@ -385,16 +486,18 @@ inline cudaError_t ozaki_gemm(const OzakiOperand& A, bool a_shared, const OzakiO
         if (e != cudaSuccess) return e;
         attr_set[dev] = true;
     }
-    if (A.Kp != B.Kp || A.Rp % BM != 0 || B.Rp % BN != 0 || A.K > kMaxK || (!a_shared && A.batch != B.batch))
+    const int batch = a_shared ? B.batch : A.batch;
+    if (A.Kp != B.Kp || A.Kp <= 0 || A.Rp % BM != 0 || B.Rp % BN != 0 || A.K > kMaxK ||
+        (!a_shared && !b_shared && A.batch != B.batch) || (a_shared && b_shared && batch != 1))
         return cudaErrorInvalidValue;
     OzakiArgs p{};
     p.A = A.q;  p.a_batch = a_shared ? 0 : (long long)operand_bytes(A.Rp, A.Kp);
     p.RpA = A.Rp;  p.eA = A.e;  p.ea_batch = a_shared ? 0 : A.Rp;
-    p.B = B.q;  p.b_batch = (long long)operand_bytes(B.Rp, B.Kp);
-    p.RpB = B.Rp;  p.eB = B.e;  p.eb_batch = B.Rp;
+    p.B = B.q;  p.b_batch = b_shared ? 0 : (long long)operand_bytes(B.Rp, B.Kp);
+    p.RpB = B.Rp;  p.eB = B.e;  p.eb_batch = b_shared ? 0 : B.Rp;
     p.Kp = A.Kp;
     p.M = (int)A.R;  p.N = (int)B.R;
-    p.nmb = (int)(A.Rp / BM);  p.nnb = (int)(B.Rp / BN);  p.batch = B.batch;
+    p.nmb = (int)(A.Rp / BM);  p.nnb = (int)(B.Rp / BN);  p.batch = batch;
     p.C = C;  p.ldc = ldc;  p.c_batch = c_batch;
     p.alpha = alpha;  p.beta = beta;
     p.err = err;

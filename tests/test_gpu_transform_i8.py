@@ -93,3 +93,48 @@ def test_mixed_energy_with_int8_transform_vs_fp64(ctx):
     e3 = ctx.mp2_energy(capi.RESTRICTED, capi.FP16X3)
     e64 = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)
     assert abs(e3["total"] - e64["total"]) <= 1e-6
+
+
+# The backward's transposed transforms of the mixed path run on the same
+# int8 products (dC_vir over batches of occupied orbitals, W with C_vir
+# shared, dC_occ over batches of Q).  dE/dC agrees with the FP64 path to the
+# mixed-path tolerance 1e-6, with stored vectors, generated vectors in one
+# chunk or in chunks of 7, and with the int8 transforms switched off.
+def twin_inputs(N, o, M, seed):
+    base = syn.make_inputs(N, o, M, seed=seed)
+    sig = syn.twin_sigma(N, o, M, base.alpha.eps)
+    return syn.make_inputs(N, o, M, seed=seed, sigma=sig)
+
+
+@pytest.mark.parametrize("switch", [None, "f64"])
+def test_mixed_gradient_int8_transposed_vs_fp64(ctx, monkeypatch, switch):
+    N, o, M = 150, 17, 380
+    inp = twin_inputs(N, o, M, seed=21)
+    a = inp.alpha
+    ctx.set_vectors(inp.L).set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    g64 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
+    if switch:
+        monkeypatch.setenv("MSHQC_CD_TRANSFORM", switch)
+    ctx.set_orbitals(capi.ALPHA, a.C, a.eps, o)
+    g3 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
+    assert abs(g3.energy["total"] - g64.energy["total"]) <= 1e-6
+    assert np.max(np.abs(g3.dC_a - g64.dC_a)) <= 1e-6
+    assert np.max(np.abs(g3.deps_a - g64.deps_a)) <= 1e-6
+
+
+@pytest.mark.parametrize("chunk", [None, "7"])
+def test_generated_mixed_gradient_vs_fp64(monkeypatch, chunk):
+    N, o, M, seed = 64, 8, 150, 4
+    if chunk:
+        monkeypatch.setenv("MSHQC_CD_GEN_CHUNK", chunk)
+    orb = syn.make_orbitals(N, o, 7)
+    sigma = syn.twin_sigma(N, o, M, orb.eps)
+    out = {}
+    for prec in (capi.FP64, capi.FP16X3):
+        with capi.Context(0) as c:
+            c.gen_vectors(N, M, seed, sigma)
+            c.set_orbitals(capi.ALPHA, orb.C, orb.eps, o)
+            out[prec] = c.mp2_gradient(capi.RESTRICTED, prec)
+    g64, g3 = out[capi.FP64], out[capi.FP16X3]
+    assert abs(g3.energy["total"] - g64.energy["total"]) <= 1e-6
+    assert np.max(np.abs(g3.dC_a - g64.dC_a)) <= 1e-6
