@@ -49,8 +49,8 @@ struct AmpElemArgs {
     double wgt;             // weight of the pair sums (2 when the mirror block (J, I) is skipped)
     const double* eox; const double* evx;   // energies of the row spin
     const double* eoy; const double* evy;   // of the column spin
-    uint16_t* Ahi; uint16_t* Alo; long long RA;   // SPLIT: rows R = ii*rsx + a, K = jj*ksy + b
-    uint16_t* Thi; uint16_t* Tlo; long long RT;   // SPLIT, optional transpose: rows jj*ksy + b, K = ii*rsx + a
+    uint16_t* Ahi; uint16_t* Alo; long long nkA;  // SPLIT: rows R = ii*rsx + a, K = jj*ksy + b (nkA = K / 16)
+    uint16_t* Thi; uint16_t* Tlo; long long nkT;  // SPLIT, optional transpose: rows jj*ksy + b, K = ii*rsx + a
     double* A64; long long ldA;                   // FP64: [R][K], K = jj*ksy + b
     double* partial;        // [ox * oy] energy of each pair (i, j), i over all row orbitals
     double* prow;           // [ox * oy][rsx] sum_b r per pair and row a (or null)
@@ -59,10 +59,13 @@ struct AmpElemArgs {
 };
 
 namespace amp_detail {
-// blocked K-major element offset of (row R, column k): 16-wide K chunks of
-// RA rows, 8 x 8 core matrices (the operand layout of the Gamma kernel)
-__device__ __forceinline__ long long blocked_offset(long long R, long long k, long long RA) {
-    return (k >> 4) * RA * 16 + ((R >> 3) * 16 + ((k & 15) >> 3) * 8 + (R & 7)) * 8 + (k & 7);
+// blocked K-major element offset of (row R, column k) in the operand layout
+// of the Gamma kernel: 128-row blocks, each holding its nkc 16-wide K chunks
+// one after the other (so consecutive K chunks of a tile are one copy), 8 x 8
+// core matrices inside a 128 x 16 chunk
+__device__ __forceinline__ long long blocked_offset(long long R, long long k, long long nkc) {
+    return ((R >> 7) * nkc + (k >> 4)) * 2048 + (((R & 127) >> 3) * 16 + ((k & 15) >> 3) * 8 + (R & 7)) * 8 +
+           (k & 7);
 }
 
 // eight consecutive-k values -> one 16-byte hi row and one 16-byte lo row
@@ -157,14 +160,14 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                     const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
                     const long long R = (long long)ii * p.rsx + a0 + r;
                     const long long kc = (long long)jj * p.ksy + b0 + g * 8;
-                    const long long off = amp_detail::blocked_offset(R, kc, p.RA);
+                    const long long off = amp_detail::blocked_offset(R, kc, p.nkA);
                     amp_detail::store_hilo8(&T[r][g * 8], p.Ahi + off, p.Alo + off);
                 } else if (p.Thi) {
                     const int w = threadIdx.x - 128;
                     const int r = w >> 2, g = w & 3;   // r: b offset, g: group of 8 a
                     const long long R = (long long)jj * p.ksy + b0 + r;
                     const long long kc = (long long)ii * p.rsx + a0 + g * 8;
-                    const long long off = amp_detail::blocked_offset(R, kc, p.RT);
+                    const long long off = amp_detail::blocked_offset(R, kc, p.nkT);
                     double col[8];
 #pragma unroll
                     for (int e = 0; e < 8; ++e) col[e] = T[g * 8 + e][r];

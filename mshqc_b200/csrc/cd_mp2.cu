@@ -900,13 +900,15 @@ int make_bt(mshqc_cd_ctx* ctx, int spin, DevBuf& buf, int64_t RQ, const uint16_t
     return MSHQC_CD_OK;
 }
 
-// gamma[(i0 + R / VR, R % VR)][Q] (+)= sum_K A[R][K] BT[Q][K] for R < rows
-int launch_gamma(mshqc_cd_ctx* ctx, const uint16_t* ahi, const uint16_t* alo, int64_t RA, const uint16_t* bhi,
-                 const uint16_t* blo, int64_t RQ, int64_t K, int64_t rows, int64_t VR, int64_t v, int64_t vp,
-                 int i0, double* gamma, int accumulate) {
+// gamma[(i0 + R / VR, R % VR)][Q] (+)= sum_K A[R][K] BT[Q][K] for R < rows;
+// a_rbs / b_rbs: K chunks per row block of A (128 rows) and of BT (256 rows),
+// bhi / blo pointing at the first K chunk used
+int launch_gamma(mshqc_cd_ctx* ctx, const uint16_t* ahi, const uint16_t* alo, int64_t a_rbs, const uint16_t* bhi,
+                 const uint16_t* blo, int64_t b_rbs, int64_t RQ, int64_t K, int64_t rows, int64_t VR, int64_t v,
+                 int64_t vp, int i0, double* gamma, int accumulate) {
     GammaTcArgs g{};
     g.Ahi = ahi;  g.Alo = alo;  g.Bhi = bhi;  g.Blo = blo;
-    g.RA = RA;  g.RQ = RQ;
+    g.a_rbs = a_rbs;  g.b_rbs = b_rbs;
     g.nk = (int)(K / 16);
     g.KP = 32;
     g.nrb = (int)(rows / 128);
@@ -1035,10 +1037,10 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
             e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
             e.Ahi = ctx->amp.as<uint16_t>();  e.Alo = ctx->amp2.as<uint16_t>();
-            e.RA = (long long)bI * dx.VR;
+            e.nkA = (long long)nJ * dy.VR / 16;
             if (mirror) {
                 e.Thi = ctx->ampT.as<uint16_t>();  e.Tlo = ctx->ampT2.as<uint16_t>();
-                e.RT = (long long)bJ * dy.VR;
+                e.nkT = (long long)nI * dx.VR / 16;
             }
             e.partial = partial;
             e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
@@ -1048,14 +1050,16 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             CD_CUDA(cudaGetLastError());
             ctx->launches++;
             // Gamma_sx[I] += A x B_sy[J]  (K range of J inside the transposed B of spin sy)
-            const size_t kJ = (size_t)J0 * dy.VR * RQ, kI = (size_t)I0 * dx.VR * RQ;
-            CD_RC(launch_gamma(ctx, e.Ahi, e.Alo, e.RA, bty[0] + kJ, bty[1] + kJ, RQ, (int64_t)nJ * dy.VR,
+            // first K chunk of block J (I) inside a 256-row block of BT
+            const size_t kJ = (size_t)J0 * dy.VR / 16 * 4096, kI = (size_t)I0 * dx.VR / 16 * 4096;
+            const int64_t nkBy = dy.o * dy.VR / 16, nkBx = dx.o * dx.VR / 16;
+            CD_RC(launch_gamma(ctx, e.Ahi, e.Alo, e.nkA, bty[0] + kJ, bty[1] + kJ, nkBy, RQ, (int64_t)nJ * dy.VR,
                                (int64_t)nI * dx.VR, dx.VR, dx.v, dx.vp, (int)I0, ctx->gam[sx].as<double>(), 1));
             if (mirror) {
                 // Gamma_sy[J] += A^T x B_sx[I]
-                CD_RC(launch_gamma(ctx, e.Thi, e.Tlo, e.RT, btx[0] + kI, btx[1] + kI, RQ, (int64_t)nI * dx.VR,
-                                   (int64_t)nJ * dy.VR, dy.VR, dy.v, dy.vp, (int)J0, ctx->gam[sy].as<double>(),
-                                   1));
+                CD_RC(launch_gamma(ctx, e.Thi, e.Tlo, e.nkT, btx[0] + kI, btx[1] + kI, nkBx, RQ,
+                                   (int64_t)nI * dx.VR, (int64_t)nJ * dy.VR, dy.VR, dy.v, dy.vp, (int)J0,
+                                   ctx->gam[sy].as<double>(), 1));
             }
         }
     }

@@ -4,9 +4,15 @@
 //
 // A operand: the amplitude operand written by amp_elem.cuh (rows (i - i0, a),
 // K = (j, b)); B operand: BT, the MO vectors transposed to rows Q, K = (j, b).
-// Both are BF16 hi/lo pairs in the blocked K-major layout of pair_energy_tc.cuh
-// (element (r, k) of a matrix with R rows
-// at (k/16)*R*16 + (r/8*16 + (k%16)/8*8 + r%8)*8 + k%8).
+// Both are BF16 hi/lo pairs in a row-block-major blocked K-major layout: the
+// matrix is cut into blocks of BR rows (128 for A, 256 for B), each block
+// stores its 16-wide K chunks one after the other (BR x 16 elements each,
+// 8 x 8 core matrices inside), so element (r, k) sits at
+//   ((r / BR) * nkc + k / 16) * BR * 16 + ((r % BR) / 8 * 16 + (k % 16) / 8 * 8 + r % 8) * 8 + k % 8
+// with nkc the K chunks per block (a_rbs, b_rbs).  Consecutive K steps of a
+// tile are contiguous, so one bulk copy moves KS = 2 steps: the copies of a
+// 128 x 256 tile are feed-bound at one step per copy (measured: 10.1 ms for a
+// launch whose MMAs alone take 7.3 ms; 7.7 ms with two steps per copy).
 //
 // Tile 128 rows x 256 Q; per 16-wide K step three 128x256x16 MMAs
 // (hi.hi + hi.lo + lo.hi).  The K range is cut into chunks of KP steps that
@@ -28,10 +34,10 @@
 namespace mshqc_cd {
 
 struct GammaTcArgs {
-    const uint16_t* Ahi; const uint16_t* Alo;   // staging, RA rows
-    const uint16_t* Bhi; const uint16_t* Blo;   // BT, RQ rows
-    long long RA, RQ;
-    int nk;                 // K steps of 16 (K = o * VR)
+    const uint16_t* Ahi; const uint16_t* Alo;   // staging (128-row blocks of a_rbs K chunks)
+    const uint16_t* Bhi; const uint16_t* Blo;   // BT from the first K chunk used (256-row blocks of b_rbs chunks)
+    long long a_rbs, b_rbs;
+    int nk;                 // K steps of 16 (even)
     int KP;                 // K steps per promotion chunk
     int nrb, nqb;           // row blocks (of 128) and Q blocks (of 256) to compute
     int VR, v, vp, Mp, i0;  // output mapping R -> (i0 + R / VR, R % VR)
@@ -41,12 +47,12 @@ struct GammaTcArgs {
 };
 
 namespace gamma_tc {
-constexpr int BM = 128, BN = 256, KC = 16, STAGES = 8, THREADS = 576, EPI_WARPS = 16;
-constexpr uint32_t SLAB_A = BM * KC * 2;        // 4 KB
-constexpr uint32_t SLAB_B = BN * KC * 2;        // 8 KB
-constexpr uint32_t OFF_AH = 0, OFF_AL = SLAB_A, OFF_BH = 2 * SLAB_A, OFF_BL = 2 * SLAB_A + SLAB_B;
-constexpr uint32_t STAGE_BYTES = 2 * (SLAB_A + SLAB_B);   // 24 KB
-constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;      // 192 KB
+constexpr int BM = 128, BN = 256, KC = 16, KS = 2, STAGES = 4, THREADS = 576, EPI_WARPS = 16;
+constexpr uint32_t SLAB_A = BM * KC * 2;        // 4 KB per K step
+constexpr uint32_t SLAB_B = BN * KC * 2;        // 8 KB per K step
+constexpr uint32_t OFF_AH = 0, OFF_AL = KS * SLAB_A, OFF_BH = 2 * KS * SLAB_A, OFF_BL = 2 * KS * SLAB_A + KS * SLAB_B;
+constexpr uint32_t STAGE_BYTES = KS * 2 * (SLAB_A + SLAB_B);   // 48 KB: KS steps
+constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;           // 192 KB
 constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 + 256;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 constexpr uint32_t TMEM_COLS = 512;
@@ -98,8 +104,8 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
             uint32_t fill_phase = 0, filled = 0;   // bit s: parity / presence of stage s's last fill
             for (long long u = first; u < units && !*abort_flag; u += step) {
                 const long long rb = u / p.nqb, qb = u % p.nqb;
-                const size_t ra0 = (size_t)rb * BM * 16, rq0 = (size_t)qb * BN * 16;
-                for (int kq = 0; kq < p.nk; ++kq) {
+                const size_t ra0 = (size_t)rb * p.a_rbs * (BM * 16), rq0 = (size_t)qb * p.b_rbs * (BN * 16);
+                for (int kq = 0; kq < p.nk; kq += KS) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
                         atomicExch(p.err, 11);
                         *abort_flag = 1;
@@ -107,11 +113,11 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
                     }
                     uint8_t* sb = smem + stage * STAGE_BYTES;
                     mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-                    const size_t ka = (size_t)kq * p.RA * 16, kb = (size_t)kq * p.RQ * 16;
-                    bulk_g2s(sb + OFF_AH, p.Ahi + ka + ra0, SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_AL, p.Alo + ka + ra0, SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_BH, p.Bhi + kb + rq0, SLAB_B, &full[stage]);
-                    bulk_g2s(sb + OFF_BL, p.Blo + kb + rq0, SLAB_B, &full[stage]);
+                    const size_t ka = ra0 + (size_t)kq * (BM * 16), kb = rq0 + (size_t)kq * (BN * 16);
+                    bulk_g2s(sb + OFF_AH, p.Ahi + ka, KS * SLAB_A, &full[stage]);
+                    bulk_g2s(sb + OFF_AL, p.Alo + ka, KS * SLAB_A, &full[stage]);
+                    bulk_g2s(sb + OFF_BH, p.Bhi + kb, KS * SLAB_B, &full[stage]);
+                    bulk_g2s(sb + OFF_BL, p.Blo + kb, KS * SLAB_B, &full[stage]);
                     fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
                     filled |= 1u << stage;
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
@@ -148,7 +154,7 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
                     tc_fence_after();
                     const uint32_t d = tmem + buf * BN;
                     const int kend = min(p.nk, kq + p.KP);
-                    for (int ks = 0; kq < kend; ++kq, ++ks) {
+                    for (int ks = 0; kq < kend; kq += KS, ks += KS) {
                         if (!mbar_wait_bounded(&full[stage], phase, kWaitLimitNs)) {
                             atomicExch(p.err, 13);
                             *abort_flag = 1;
@@ -156,13 +162,16 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
                         }
                         tc_fence_after();
                         const uint32_t sb = sbase + stage * STAGE_BYTES;
-                        const uint64_t ah = smem_desc_kmajor(sb + OFF_AH, 128, 256);
-                        const uint64_t al = smem_desc_kmajor(sb + OFF_AL, 128, 256);
-                        const uint64_t bh = smem_desc_kmajor(sb + OFF_BH, 128, 256);
-                        const uint64_t bl = smem_desc_kmajor(sb + OFF_BL, 128, 256);
-                        mma_f16(d, ah, bh, IDESC, ks > 0 ? 1u : 0u);
-                        mma_f16(d, ah, bl, IDESC, 1u);
-                        mma_f16(d, al, bh, IDESC, 1u);
+#pragma unroll
+                        for (int j = 0; j < KS; ++j) {
+                            const uint64_t ah = smem_desc_kmajor(sb + OFF_AH + j * SLAB_A, 128, 256);
+                            const uint64_t al = smem_desc_kmajor(sb + OFF_AL + j * SLAB_A, 128, 256);
+                            const uint64_t bh = smem_desc_kmajor(sb + OFF_BH + j * SLAB_B, 128, 256);
+                            const uint64_t bl = smem_desc_kmajor(sb + OFF_BL + j * SLAB_B, 128, 256);
+                            mma_f16(d, ah, bh, IDESC, (ks + j) > 0 ? 1u : 0u);
+                            mma_f16(d, ah, bl, IDESC, 1u);
+                            mma_f16(d, al, bh, IDESC, 1u);
+                        }
                         mma_commit(&empty[stage]);
                         if (++stage == STAGES) { stage = 0; phase ^= 1; }
                     }
@@ -233,7 +242,9 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
 }
 
 // MO vectors B[j][b][Q] (FP64, [o][vp][Mp]) -> BT hi/lo BF16 with rows Q
-// (RQ rows), K = (j, b) with b padded to VR; zeros outside b < v, Q < M.
+// (RQ rows, a multiple of 256), K = (j, b) with b padded to VR; zeros outside
+// b < v, Q < M.  Layout: 256-row blocks of o * VR / 16 K chunks (the B
+// operand layout of gamma_tc_kernel).
 static __global__ void bt_split_kernel(const double* __restrict__ B, int64_t vp, int64_t Mp, int v, int M,
                                        int64_t o, int64_t VR, int64_t RQ, uint16_t* __restrict__ hi,
                                        uint16_t* __restrict__ lo) {
@@ -259,7 +270,7 @@ static __global__ void bt_split_kernel(const double* __restrict__ B, int64_t vp,
             h[e] = __bfloat16_as_ushort(bh);
             l[e] = __bfloat16_as_ushort(bl);
         }
-        const int64_t off = t * 8;   // == kc*RQ*16 + (g*16 + kk*8 + r)*8
+        const int64_t off = ((g >> 5) * nkc + kc) * 4096 + ((g & 31) * 16 + kk * 8 + r) * 8;
         uint4 vh, vl;
         vh.x = h[0] | (uint32_t(h[1]) << 16); vh.y = h[2] | (uint32_t(h[3]) << 16);
         vh.z = h[4] | (uint32_t(h[5]) << 16); vh.w = h[6] | (uint32_t(h[7]) << 16);
