@@ -3,11 +3,13 @@
 //
 // Operands live in a "core-matrix blocked" layout so that every operand slab
 // is one contiguous run of bytes that lands in shared memory already in the
-// canonical K-major no-swizzle UMMA layout:
+// canonical K-major no-swizzle UMMA layout (split_bf16.cuh):
 //
-//   element (i, a, Q) at  (i*nqc + Q/16)*rows*16 + (a/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
+//   element (i, a, Q) at  ((i*rows/256 + a/256)*nqc + Q/16)*4096
+//                         + ((a%256)/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
 //
-// A slab = rows [a0, a0+128) x one 16-wide Q chunk = 4 KB contiguous.
+// A slab = rows [a0, a0+128) x one 16-wide Q chunk = 4 KB contiguous; the
+// slabs of consecutive chunks are 8 KB apart.
 //
 // Work unit = pair (i,j), row block x (128 virtuals a), column block y (128
 // virtuals b).  Per Q chunk the MMA thread issues six 128x128x16 MMAs into
@@ -149,25 +151,24 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             for (long long u = first; u < p.units && !*abort_flag; u += step) {
                 const int2 ij = p.pairs[u / p.nblocks];
                 const int2 xy = p.blocks[u % p.nblocks];
-                const size_t rx = p.rows_x, ry = p.rows_y;
                 const size_t a0 = (size_t)xy.x * BM, b0 = (size_t)xy.y * BN;
-                // slab bases at Q chunk 0; chunk kq adds kq * rows * 16 elements
+                // slab bases at Q chunk 0 (element offset of the 128 rows from r0
+                // of orbital o); chunk kq adds kq * 4096 elements
+                const size_t nbx = (size_t)p.rows_x / 256, nby = (size_t)p.rows_y / 256, nq = (size_t)p.nqc;
+                auto slab_x = [&](size_t o, size_t r0) { return ((o * nbx + r0 / 256) * nq) * 4096 + (r0 % 256) * 16; };
+                auto slab_y = [&](size_t o, size_t r0) { return ((o * nby + r0 / 256) * nq) * 4096 + (r0 % 256) * 16; };
                 const uint16_t *s0h, *s1h, *s2h, *s3h, *s0l, *s1l, *s2l, *s3l;
-                size_t c0, c1, c2, c3;
+                const size_t c0 = 4096, c1 = 4096, c2 = 4096, c3 = 4096;
                 if (MODE == PAIR_OPPOSITE_SPIN) {
-                    const size_t oi = (size_t)ij.x * p.nqc * rx * 16, oj = (size_t)ij.y * p.nqc * ry * 16;
-                    s0h = p.Xhi + oi + a0 * 16;         s0l = p.Xlo + oi + a0 * 16;
-                    s1h = p.Yhi + oj + b0 * 16;         s1l = p.Ylo + oj + b0 * 16;
-                    s2h = s0h;                          s2l = s0l;
-                    s3h = p.Yhi + oj + (b0 + BN) * 16;  s3l = p.Ylo + oj + (b0 + BN) * 16;
-                    c0 = rx * 16; c1 = ry * 16; c2 = c0; c3 = ry * 16;
+                    s0h = p.Xhi + slab_x(ij.x, a0);       s0l = p.Xlo + slab_x(ij.x, a0);
+                    s1h = p.Yhi + slab_y(ij.y, b0);       s1l = p.Ylo + slab_y(ij.y, b0);
+                    s2h = s0h;                            s2l = s0l;
+                    s3h = p.Yhi + slab_y(ij.y, b0 + BN);  s3l = p.Ylo + slab_y(ij.y, b0 + BN);
                 } else {
-                    const size_t oi = (size_t)ij.x * p.nqc * rx * 16, oj = (size_t)ij.y * p.nqc * rx * 16;
-                    s0h = p.Xhi + oi + a0 * 16;  s0l = p.Xlo + oi + a0 * 16;
-                    s1h = p.Xhi + oj + b0 * 16;  s1l = p.Xlo + oj + b0 * 16;
-                    s2h = p.Xhi + oj + a0 * 16;  s2l = p.Xlo + oj + a0 * 16;
-                    s3h = p.Xhi + oi + b0 * 16;  s3l = p.Xlo + oi + b0 * 16;
-                    c0 = c1 = c2 = c3 = rx * 16;
+                    s0h = p.Xhi + slab_x(ij.x, a0);  s0l = p.Xlo + slab_x(ij.x, a0);
+                    s1h = p.Xhi + slab_x(ij.y, b0);  s1l = p.Xlo + slab_x(ij.y, b0);
+                    s2h = p.Xhi + slab_x(ij.y, a0);  s2l = p.Xlo + slab_x(ij.y, a0);
+                    s3h = p.Xhi + slab_x(ij.x, b0);  s3l = p.Xlo + slab_x(ij.x, b0);
                 }
                 const uint32_t bytes = (MODE == PAIR_OPPOSITE_SPIN) ? 6 * SLAB : 8 * SLAB;
                 for (int kq = 0; kq < nk; ++kq) {

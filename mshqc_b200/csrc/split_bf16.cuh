@@ -99,7 +99,12 @@ static __global__ void row_scale_kernel(const double* __restrict__ src, int64_t 
 }
 
 // src: [o][vp][Mp] FP64 (zeros outside v x M); expo from row_scale_kernel.
-// dst: [o][nqc][rows][16] FP16 bits, blocked as (a/8, (Q%16)/8, a%8, Q%8).
+// dst: FP16 bits in 256-row blocks, each holding its nqc 16-wide Q chunks one
+// after the other, blocked inside a chunk as (a/8, (Q%16)/8, a%8, Q%8):
+//   element (i, a, Q) at ((i*rows/256 + a/256)*nqc + Q/16)*4096
+//                        + ((a%256)/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
+// (rows a multiple of 256), so a 128-row slab of one chunk is 4 KB and a
+// 256-row slab of consecutive chunks is one contiguous run.
 static __global__ void split_fixed_blocked_kernel(const double* __restrict__ src, int64_t vp,
                                                   int64_t Mp, int v, int M, int64_t o, int64_t nqc,
                                                   int64_t rows, const int* __restrict__ expo,
@@ -130,7 +135,7 @@ static __global__ void split_fixed_blocked_kernel(const double* __restrict__ src
             h[k] = __half_as_ushort(__double2half(hv));   // exact: |hv| <= 1024
             l[k] = __half_as_ushort(__double2half(lv));   // exact: |lv| <= 128
         }
-        const int64_t off = t * 8;   // == iq*rows*16 + (g*16 + kk*8 + r)*8
+        const int64_t off = ((i * (rows / 256) + (g >> 5)) * nqc + qc) * 4096 + ((g & 31) * 16 + kk * 8 + r) * 8;
         uint4 vh, vl;
         vh.x = h[0] | (uint32_t(h[1]) << 16); vh.y = h[2] | (uint32_t(h[3]) << 16);
         vh.z = h[4] | (uint32_t(h[5]) << 16); vh.w = h[6] | (uint32_t(h[7]) << 16);

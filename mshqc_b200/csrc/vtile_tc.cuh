@@ -6,8 +6,11 @@
 // j), every tile computed once;
 // X and Y are the MO vectors of one spin (restricted, same spin) or of the
 // two spins (opposite spin: X alpha, Y beta).
-// Operands are the exact fixed-point hi/lo of split_bf16.cuh in the blocked
-// layout of pair_energy_tc.cuh; per 16-wide Q step three 128x256x16 MMAs
+// Operands are the exact fixed-point hi/lo of split_bf16.cuh in its 256-row
+// blocked layout; a stage holds KS = 2 Q steps: the A slab (128 rows) per
+// step, the B slab (256 rows) of both steps in one copy (one-step copies
+// left the kernel feed-bound: 7.7 ms for a launch whose MMAs take 5.8 ms;
+// 5.9 ms with the two-step B copies).  Per 16-wide Q step three 128x256x16 MMAs
 // accumulate the hi*hi' and the hi*lo' + lo*hi' integers exactly in two TMEM
 // accumulators (columns [0,256) and [256,512)), and the epilogue recovers
 //   (ia|jb) = u_ia u_jb (hh + x / 256)
@@ -42,12 +45,12 @@ struct VtileArgs {
 };
 
 namespace vtile_tc {
-constexpr int BM = 128, BN = 256, KC = 16, STAGES = 8, THREADS = 192;
-constexpr uint32_t SLAB_A = BM * KC * 2;     // 4 KB
-constexpr uint32_t SLAB_B = BN * KC * 2;     // 8 KB
-constexpr uint32_t OFF_AH = 0, OFF_AL = SLAB_A, OFF_BH = 2 * SLAB_A, OFF_BL = 2 * SLAB_A + SLAB_B;
-constexpr uint32_t STAGE_BYTES = 2 * (SLAB_A + SLAB_B);   // 24 KB
-constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;      // 192 KB
+constexpr int BM = 128, BN = 256, KC = 16, KS = 2, STAGES = 4, THREADS = 192;
+constexpr uint32_t SLAB_A = BM * KC * 2;     // 4 KB per Q step
+constexpr uint32_t SLAB_B = BN * KC * 2;     // 8 KB per Q step
+constexpr uint32_t OFF_AH = 0, OFF_AL = KS * SLAB_A, OFF_BH = 2 * KS * SLAB_A, OFF_BL = 2 * KS * SLAB_A + KS * SLAB_B;
+constexpr uint32_t STAGE_BYTES = KS * 2 * (SLAB_A + SLAB_B);   // 48 KB
+constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;           // 192 KB
 constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 + 256 + BN * 8;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 constexpr uint32_t TMEM_COLS = 512;
@@ -101,24 +104,30 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
                 const long long pr = u / per_pair, bb = u % per_pair;
                 const int i = p.i0 + (int)(pr / p.nbj), j = p.j0 + (int)(pr % p.nbj);
                 const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
-                const size_t rx = p.rows_x, ry = p.rows_y;
-                const uint16_t* ah = p.Xhi + (size_t)i * p.nqc * rx * 16 + (size_t)x * BM * 16;
-                const uint16_t* al = p.Xlo + (size_t)i * p.nqc * rx * 16 + (size_t)x * BM * 16;
-                const uint16_t* bh = p.Yhi + (size_t)j * p.nqc * ry * 16 + (size_t)y * BN * 16;
-                const uint16_t* bl = p.Ylo + (size_t)j * p.nqc * ry * 16 + (size_t)y * BN * 16;
-                for (int kq = 0; kq < nk; ++kq) {
+                // slab bases at Q step 0 (256-row blocks of nqc steps, 4096 elements a step)
+                const size_t nq = (size_t)p.nqc;
+                const size_t xa = (((size_t)i * (p.rows_x / 256) + x / 2) * nq) * 4096 + (size_t)(x % 2) * 2048;
+                const size_t yb = (((size_t)j * (p.rows_y / 256) + y) * nq) * 4096;
+                const uint16_t* ah = p.Xhi + xa;
+                const uint16_t* al = p.Xlo + xa;
+                const uint16_t* bh = p.Yhi + yb;
+                const uint16_t* bl = p.Ylo + yb;
+                for (int kq = 0; kq < nk; kq += KS) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
                         atomicExch(p.err, 21);
                         *abort_flag = 1;
                         break;
                     }
+                    const int nks = min(KS, nk - kq);
                     uint8_t* sb = smem + stage * STAGE_BYTES;
-                    mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-                    const size_t kx = (size_t)kq * rx * 16, ky = (size_t)kq * ry * 16;
-                    bulk_g2s(sb + OFF_AH, ah + kx, SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_AL, al + kx, SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_BH, bh + ky, SLAB_B, &full[stage]);
-                    bulk_g2s(sb + OFF_BL, bl + ky, SLAB_B, &full[stage]);
+                    mbar_arrive_expect_tx(&full[stage], (uint32_t)nks * 2 * (SLAB_A + SLAB_B));
+                    const size_t kk = (size_t)kq * 4096;
+                    for (int q2 = 0; q2 < nks; ++q2) {
+                        bulk_g2s(sb + OFF_AH + q2 * SLAB_A, ah + kk + q2 * 4096, SLAB_A, &full[stage]);
+                        bulk_g2s(sb + OFF_AL + q2 * SLAB_A, al + kk + q2 * 4096, SLAB_A, &full[stage]);
+                    }
+                    bulk_g2s(sb + OFF_BH, bh + kk, nks * SLAB_B, &full[stage]);
+                    bulk_g2s(sb + OFF_BL, bl + kk, nks * SLAB_B, &full[stage]);
                     fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
                     filled |= 1u << stage;
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
@@ -150,7 +159,7 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
                 }
                 acc_phase ^= 1;
                 tc_fence_after();
-                for (int kq = 0; kq < nk; ++kq) {
+                for (int kq = 0; kq < nk; kq += KS) {
                     if (!mbar_wait_bounded(&full[stage], phase, kWaitLimitNs)) {
                         atomicExch(p.err, 23);
                         *abort_flag = 1;
@@ -158,14 +167,17 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
                     }
                     tc_fence_after();
                     const uint32_t sb = sbase + stage * STAGE_BYTES;
-                    const uint64_t ah = smem_desc_kmajor(sb + OFF_AH, 128, 256);
-                    const uint64_t al = smem_desc_kmajor(sb + OFF_AL, 128, 256);
-                    const uint64_t bh = smem_desc_kmajor(sb + OFF_BH, 128, 256);
-                    const uint64_t bl = smem_desc_kmajor(sb + OFF_BL, 128, 256);
-                    const uint32_t acc = kq > 0 ? 1u : 0u;
-                    mma_f16(tmem, ah, bh, IDESC, acc);
-                    mma_f16(tmem + BN, ah, bl, IDESC, acc);
-                    mma_f16(tmem + BN, al, bh, IDESC, 1u);
+                    const int nks = min(KS, nk - kq);
+                    for (int q2 = 0; q2 < nks; ++q2) {
+                        const uint64_t ah = smem_desc_kmajor(sb + OFF_AH + q2 * SLAB_A, 128, 256);
+                        const uint64_t al = smem_desc_kmajor(sb + OFF_AL + q2 * SLAB_A, 128, 256);
+                        const uint64_t bh = smem_desc_kmajor(sb + OFF_BH + q2 * SLAB_B, 128, 256);
+                        const uint64_t bl = smem_desc_kmajor(sb + OFF_BL + q2 * SLAB_B, 128, 256);
+                        const uint32_t acc = (kq + q2) > 0 ? 1u : 0u;
+                        mma_f16(tmem, ah, bh, IDESC, acc);
+                        mma_f16(tmem + BN, ah, bl, IDESC, acc);
+                        mma_f16(tmem + BN, al, bh, IDESC, 1u);
+                    }
                     mma_commit(&empty[stage]);
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
