@@ -22,7 +22,8 @@
 // pass, or, for the symmetric modes (t^{ji}_{ba} = t^{ij}_{ab}), the rows j of
 // a block pair (I, J) whose mirror (J, I) is not computed.
 // One CTA of 256 threads takes one pair (i, j) and walks its 32 x 32 tiles of
-// (a, b), column block outer; the pair's energy, its row sums
+// (a, b), row block outer, loading the next tile while it works on the
+// current one; the pair's energy, its row sums
 // sum_b r (per a), column sums sum_a r (per b) and total sum r go to per-pair
 // buffers, each written by one thread, and deps_*_kernel turn them into
 // dE/de (+r on a and b, -r on i and j) in a fixed order.
@@ -33,6 +34,7 @@
 #include <type_traits>
 
 #include "cd_common.cuh"
+#include "sm100_ptx.cuh"
 
 namespace mshqc_cd {
 
@@ -87,8 +89,9 @@ __device__ __forceinline__ void store_hilo8(const double* t, uint16_t* hi, uint1
 template <int MODE, bool SPLIT>
 __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
     using TS = typename std::conditional<SPLIT, float, double>::type;
+    constexpr bool kW = MODE != AMP_OPPOSITE_SPIN;   // (ib|ja) needed
     __shared__ TS Vt[32][33];
-    __shared__ TS Wt[MODE == AMP_OPPOSITE_SPIN ? 1 : 32][33];
+    __shared__ TS Wt[kW ? 32 : 1][33];
     __shared__ double T[32][33];
     __shared__ double colpart[8][33];
     __shared__ double red_e[8], red_r[8];
@@ -101,19 +104,40 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
     const double eij = p.eox[i] + p.eoy[j];
     double* prow = p.prow ? p.prow + pair * p.rsx : nullptr;
     double* pcol = p.pcol ? p.pcol + pair * p.ksy : nullptr;
-    double esum = 0.0, rtot = 0.0;
-    for (int yb = 0; yb < tb; ++yb) {
-        const int b0 = yb * 32;
-        double cpart = 0.0;   // column b0 + tx over this thread's rows of every row block
-        for (int xb = 0; xb < ta; ++xb) {
-            const int a0 = xb * 32;
+    const TS* Srow = S + (long long)ii * p.rsx * p.ldS + (long long)jj * p.csy;
+    // this thread's four elements of tile (a0, b0): rows ty + 8k, column tx
+    // (V); the transposed tile (b0, a0) for W
+    auto load_tile = [&](int a0, int b0, TS (&v)[4], TS (&w)[4]) {
 #pragma unroll
-            for (int r = ty; r < 32; r += 8) {
-                Vt[r][tx] = S[((long long)ii * p.rsx + a0 + r) * p.ldS + (long long)jj * p.csy + b0 + tx];
-                if (MODE != AMP_OPPOSITE_SPIN)   // (ib|ja): rows (i, b), columns (j, a)
-                    Wt[r][tx] = S[((long long)ii * p.rsx + b0 + r) * p.ldS + (long long)jj * p.csy + a0 + tx];
+        for (int k = 0; k < 4; ++k) {
+            const int r = ty + 8 * k;
+            v[k] = Srow[(long long)(a0 + r) * p.ldS + b0 + tx];
+            if (kW) w[k] = Srow[(long long)(b0 + r) * p.ldS + a0 + tx];
+        }
+    };
+    TS vn[4], wn[4];
+    load_tile(0, 0, vn, wn);
+    double esum = 0.0, rtot = 0.0;
+    // row blocks outer, column blocks inner: a thread's rows stay fixed over
+    // the inner loop, so their sums over b stay in registers; the column sums
+    // of a tile are reduced across the warps and added to pcol in xb order
+    for (int xb = 0; xb < ta; ++xb) {
+        const int a0 = xb * 32;
+        double rsum[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int yb = 0; yb < tb; ++yb) {
+            const int b0 = yb * 32;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                Vt[ty + 8 * k][tx] = vn[k];
+                if (kW) Wt[ty + 8 * k][tx] = wn[k];
             }
+            // the next tile's loads overlap this tile's arithmetic and stores
+            if (yb + 1 < tb)
+                load_tile(a0, b0 + 32, vn, wn);
+            else if (xb + 1 < ta)
+                load_tile(a0 + 32, 0, vn, wn);
             __syncthreads();
+            double cp = 0.0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int r = ty * 4 + k;
@@ -123,7 +147,7 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                     const double D = eij - p.evx[a] - p.evy[b];
                     if (fabs(D) >= kDenomSkip) {
                         const double V = (double)Vt[r][tx];
-                        const double rD = 1.0 / D;
+                        const double rD = SPLIT ? sm100::recip_nr(D) : 1.0 / D;
                         if (MODE == AMP_RESTRICTED) {
                             const double W = (double)Wt[tx][r];
                             const double t = V * rD;
@@ -144,17 +168,14 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                     }
                 }
                 T[r][tx] = amp;
-                rtot += rr;
-                cpart += rr;
-                double rs = rr;
-#pragma unroll
-                for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
-                // row a is always summed by lane 0 of warp ty: single writer, program order
-                if (prow && tx == 0) prow[a] = (yb == 0 ? 0.0 : prow[a]) + p.wgt * rs;
+                rsum[k] += rr;
+                cp += rr;
                 if (!SPLIT) p.A64[((long long)ii * p.rsx + a) * p.ldA + (long long)jj * p.ksy + b] = amp;
             }
+            rtot += cp;
+            colpart[ty][tx] = cp;
+            __syncthreads();
             if (SPLIT) {
-                __syncthreads();
                 // 32 rows x 4 groups of 8 K = 128 core-matrix rows per operand
                 if (threadIdx.x < 128) {
                     const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
@@ -174,18 +195,22 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                     amp_detail::store_hilo8(col, p.Thi + off, p.Tlo + off);
                 }
             }
-            __syncthreads();   // Vt, Wt, T are refilled by the next tile
-        }
-        if (pcol) {
-            colpart[ty][tx] = cpart;
-            __syncthreads();
-            if (ty == 0) {
+            if (pcol && ty == 0) {
                 double c = 0.0;
 #pragma unroll
                 for (int w = 0; w < 8; ++w) c += colpart[w][tx];
-                pcol[b0 + tx] = p.wgt * c;
+                pcol[b0 + tx] = (xb == 0 ? 0.0 : pcol[b0 + tx]) + p.wgt * c;
             }
-            __syncthreads();
+            __syncthreads();   // Vt, Wt, T, colpart are refilled by the next tile
+        }
+        if (prow) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                double rs = rsum[k];
+#pragma unroll
+                for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
+                if (tx == 0) prow[a0 + ty * 4 + k] = p.wgt * rs;
+            }
         }
     }
 #pragma unroll
