@@ -28,7 +28,7 @@
 
 namespace mshqc_cd {
 
-enum PairMode { PAIR_RESTRICTED = 0, PAIR_SAME_SPIN = 1, PAIR_OPPOSITE_SPIN = 2, PAIR_AMPLITUDE = 3 };
+enum PairMode { PAIR_RESTRICTED = 0, PAIR_SAME_SPIN = 1, PAIR_OPPOSITE_SPIN = 2 };
 
 struct PairF64Args {
     const double* X;   // [ox][vpx][Mp]

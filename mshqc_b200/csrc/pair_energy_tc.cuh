@@ -26,12 +26,6 @@
 // pair_energy_f64.cuh) into partial[unit].  (ia|jb) and the amplitudes are
 // never written to memory.
 //
-// AMPLITUDE (restricted backward): ordered pairs (i in a block of occupied rows,
-// all j), all (x, y) blocks; the epilogue writes tt = (2 (ia|jb) - (ib|ja))/D
-// as a BF16 hi/lo pair into a staging matrix (row (i-i0, a), column (j, b),
-// blocked like the operands) and accumulates E = sum (ia|jb) tt and
-// dE/de (r = t tt: +r on e_a and e_b, -r on e_i and e_j).
-//
 // Warp roles (192 threads): warp 0 producer (bulk copies), warp 1 MMA issuer
 // and TMEM owner, warps 2..5 epilogue (TMEM lane quadrant = warp % 4).
 // Every wait is bounded (kWaitLimitNs); on a timeout the kernel records the
@@ -66,12 +60,6 @@ struct PairTcArgs {
     double* partial;        // [units]
     double* partial2;       // [units] RESTRICTED opposite-spin part
     int* err;               // err[0]: nonzero after a timeout; err[1]: an accumulator reached 2^24
-    // AMPLITUDE mode
-    uint16_t* amp_hi; uint16_t* amp_lo;   // staging, blocked, amp_rows x (o * VR)
-    long long amp_rows;     // bi * VR
-    int VR;                 // virtual rows per occupied orbital in the staging (multiple of 128)
-    int i0;                 // first occupied row of the block
-    double* deps;           // dE/de, occupied then virtual (atomic)
 };
 
 namespace pair_tc {
@@ -89,7 +77,7 @@ constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;         // 196608
 // per-unit column tables at +512: eps (2 x 128 doubles), column scales
 // (2 x 128 doubles)
 constexpr uint32_t OFF_AUX = 512;
-constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 /*align*/ + OFF_AUX + 8 * 128 * 8;
+constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 /*align*/ + OFF_AUX + 4 * 128 * 8;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;             // 2 s
 constexpr uint32_t TMEM_COLS = 512;
 }  // namespace pair_tc
@@ -115,7 +103,6 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
     double* red = reinterpret_cast<double*>(smem + SMEM_DATA + 256);           // 8 doubles
     double* eb_s = reinterpret_cast<double*>(smem + SMEM_DATA + OFF_AUX);      // 256
     double* cs_s = eb_s + 256;                                                 // 256
-    double* colred = cs_s + 256;                                               // 4 x 128 (AMPLITUDE)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -320,8 +307,7 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                     rs1 = pow2d(p.ex[(size_t)i * p.rows_x + a] - kFixedHiBits);
                     rs2 = pow2d(p.ex[(size_t)j * p.rows_x + a] - kFixedHiBits);
                     ta = p.eox[i] + p.eox[j] - p.evx[a];
-                    if ((MODE == PAIR_RESTRICTED || MODE == PAIR_AMPLITUDE) && i == j && a >= b0 &&
-                        a < b0 + BN) {
+                    if (MODE == PAIR_RESTRICTED && i == j && a >= b0 && a < b0 + BN) {
                         dcol1 = dcol2 = a - b0;
                         dg1 = dg2 = p.diag[(size_t)i * p.rows_x + a];
                     }
@@ -330,22 +316,16 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             double s_acc = 0.0, o_acc = 0.0;
             float amax = 0.0f;
             const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
-            constexpr int CW = (MODE == PAIR_AMPLITUDE) ? 16 : 32;   // columns per TMEM read
+            constexpr int CW = 32;   // columns per TMEM read
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += CW) {
                 uint32_t h1[CW], x1[CW], h2[CW], x2[CW];
-                double tt_row[MODE == PAIR_AMPLITUDE ? CW : 1];
-                double csum[MODE == PAIR_AMPLITUDE ? CW : 1];
                 tmem_ld<CW>(lane_base + 0 + c0, h1);
                 tmem_ld<CW>(lane_base + 128 + c0, x1);
                 tmem_ld<CW>(lane_base + 256 + c0, h2);
                 tmem_ld<CW>(lane_base + 384 + c0, x2);
                 tmem_ld_wait();
-                if (MODE == PAIR_AMPLITUDE) {
-#pragma unroll
-                    for (int k = 0; k < CW; ++k) tt_row[k] = csum[k] = 0.0;
-                }
-                if (!arow && MODE != PAIR_AMPLITUDE) continue;
+                if (!arow) continue;
 #pragma unroll
                 for (int k = 0; k < CW; ++k) {
                     const int c = c0 + k;
@@ -366,24 +346,6 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                             const double D = ta - eb_s[BN + c];
                             if (fabs(D) >= kDenomSkip) s_acc = fma(v2 * v2, recip_nr(D), s_acc);
                         }
-                    } else if (MODE == PAIR_AMPLITUDE) {
-                        double tt = 0.0;
-                        if (arow && b0 + c < p.vx) {
-                            const double D = ta - eb_s[c];
-                            if (fabs(D) >= kDenomSkip) {
-                                const double rD = recip_nr(D);
-                                tt = (2.0 * v1 - v2) * rD;
-                                const double r = v1 * rD * tt;
-                                s_acc = fma(v1, tt, s_acc);
-                                o_acc += r;
-                                csum[k] = r;
-                            } else {
-                                csum[k] = 0.0;
-                            }
-                        } else {
-                            csum[k] = 0.0;
-                        }
-                        tt_row[k] = tt;
                     } else if (b0 + c < p.vx) {
                         const double D = ta - eb_s[c];
                         if (fabs(D) >= kDenomSkip) {
@@ -399,45 +361,6 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                         }
                     }
                 }
-                if (MODE == PAIR_AMPLITUDE) {
-                    // tt (hi/lo BF16) into the staging matrix: row (i-i0, a), column (j, b)
-                    const long long R = (long long)(i - p.i0) * p.VR + xy.x * BM + row;
-                    const long long k0 = (long long)j * p.VR + b0 + c0;
-#pragma unroll
-                    for (int h = 0; h < CW / 8; ++h) {
-                        const long long k = k0 + 8 * h;
-                        const long long off =
-                            (k >> 4) * p.amp_rows * 16 + ((R >> 3) * 16 + ((k & 15) >> 3) * 8 + (R & 7)) * 8;
-                        uint32_t wh[4], wl[4];
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const double t0 = tt_row[8 * h + 2 * e], t1 = tt_row[8 * h + 2 * e + 1];
-                            const __nv_bfloat16 h0 = __double2bfloat16(t0), h1v = __double2bfloat16(t1);
-                            const __nv_bfloat16 l0 = __double2bfloat16(t0 - (double)__bfloat162float(h0));
-                            const __nv_bfloat16 l1 = __double2bfloat16(t1 - (double)__bfloat162float(h1v));
-                            wh[e] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1v) << 16);
-                            wl[e] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-                        }
-                        *reinterpret_cast<uint4*>(p.amp_hi + off) = make_uint4(wh[0], wh[1], wh[2], wh[3]);
-                        *reinterpret_cast<uint4*>(p.amp_lo + off) = make_uint4(wl[0], wl[1], wl[2], wl[3]);
-                    }
-                    // column sums of r over the 32 rows of this warp: fold the
-                    // two half warps, then a butterfly after which lane l
-                    // holds the sum of column c0 + (l % 16)
-#pragma unroll
-                    for (int k = 0; k < CW; ++k) csum[k] += __shfl_xor_sync(0xffffffffu, csum[k], 16);
-#pragma unroll
-                    for (int w = CW / 2; w >= 1; w >>= 1) {
-                        const bool upper = (lane & w) != 0;
-#pragma unroll
-                        for (int k = 0; k < w; ++k) {
-                            const double send = upper ? csum[k] : csum[k + w];
-                            const double keep = upper ? csum[k + w] : csum[k];
-                            csum[k] = keep + __shfl_xor_sync(0xffffffffu, send, w);
-                        }
-                    }
-                    if (lane < CW) colred[q * BN + c0 + lane] = csum[0];
-                }
             }
             // accumulators consumed: hand TMEM back to the MMA warp
             tc_fence_before();
@@ -445,22 +368,9 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             if (lane == 0) mbar_arrive(tmem_empty);
             if (amax >= 16777216.0f) atomicOr(p.err + 1, 1);
 
-            if (MODE == PAIR_AMPLITUDE) {
-                // dE/de: +r on the virtual of each row (a) and column (b),
-                // -sum r on both occupied orbitals of the pair
-                if (arow && o_acc != 0.0) atomicAdd(&p.deps[p.diag_o + a], o_acc);
-                asm volatile("bar.sync 1, 128;\n" ::: "memory");
-                {
-                    const int c = etid;
-                    const double cs = colred[c] + colred[BN + c] + colred[2 * BN + c] + colred[3 * BN + c];
-                    if (b0 + c < p.vx && cs != 0.0) atomicAdd(&p.deps[p.diag_o + b0 + c], cs);
-                }
-            }
             // unit weights (see pair_energy_f64.cuh)
             double tot1 = s_acc, tot2 = 0.0;
-            if (MODE == PAIR_AMPLITUDE) {
-                tot2 = o_acc;
-            } else if (MODE != PAIR_OPPOSITE_SPIN) {
+            if (MODE != PAIR_OPPOSITE_SPIN) {
                 const bool diagblk = (xy.x == xy.y);
                 if (MODE == PAIR_RESTRICTED) {
                     const double w = (diagblk ? 1.0 : 2.0) * (i < j ? 2.0 : 1.0);
@@ -483,11 +393,6 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
             if (etid == 0) {
                 p.partial[u] = ((red[0] + red[1]) + (red[2] + red[3]));
                 if (MODE == PAIR_RESTRICTED) p.partial2[u] = ((red[4] + red[5]) + (red[6] + red[7]));
-                if (MODE == PAIR_AMPLITUDE) {
-                    const double rt = (red[4] + red[5]) + (red[6] + red[7]);
-                    atomicAdd(&p.deps[i], -rt);
-                    atomicAdd(&p.deps[j], -rt);
-                }
             }
         }
     }
