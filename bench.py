@@ -51,8 +51,9 @@ WORKLOADS = {
     # smaller variants of the same step
     "cdmp2_grad_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=True, precision="fp16x3"),
     "cdmp2_grad_n600_o60_m2400": dict(N=600, o=60, M=2400, gradient=True, precision="fp16x3"),
-    # energy only (the CD-RMP2 drop-in), N=400, o=40, M=1600
+    # energy only (the CD-RMP2 drop-in), N=400, o=40, M=1600 and N=1000, o=100, M=4000
     "cdrmp2_energy_n400_o40_m1600": dict(N=400, o=40, M=1600, gradient=False, precision="fp16x3"),
+    "cdrmp2_energy_n1000_o100_m4000": dict(N=1000, o=100, M=4000, gradient=False, precision="fp16x3"),
     # differentiated CD-UMP2 (the OMP2 step): separate alpha / beta orbitals
     "cdump2_grad_n600_o60_58_m2400": dict(N=600, o=60, ob=58, M=2400, gradient=True, precision="fp16x3",
                                           kind="unrestricted"),

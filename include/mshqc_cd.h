@@ -67,6 +67,12 @@ enum mshqc_cd_kind {
 };
 
 enum mshqc_cd_layout { MSHQC_CD_LAYOUT_FULL = 0, MSHQC_CD_LAYOUT_PACKED = 1 };
+/* Where a pointer argument lives.  MSHQC_CD_DEVICE buffers are read and
+ * written in the order of the context's stream (its own non-blocking stream,
+ * or the one given to mshqc_cd_set_stream): work of another stream that
+ * produces an input must be complete (synchronize it, or give the context
+ * that stream) before the call.  Every call returns only after its device
+ * outputs are written. */
 enum mshqc_cd_where { MSHQC_CD_HOST = 0, MSHQC_CD_DEVICE = 1 };
 enum mshqc_cd_spin { MSHQC_CD_ALPHA = 0, MSHQC_CD_BETA = 1 };
 

@@ -204,6 +204,9 @@ class Context:
         if _is_torch_cuda(L):
             import torch
             L = L.to(torch.float64).contiguous()
+            # the library copies on its own stream: the conversion (and the
+            # caller's producer) on torch's current stream must be done first
+            torch.cuda.current_stream(L.device).synchronize()
             where = DEVICE
         else:
             L = _host_f64(L)
@@ -243,6 +246,9 @@ class Context:
             import torch
             Cc = C.to(torch.float64).t().contiguous()     # column-major bytes
             ec = eps.to(torch.float64).contiguous()
+            # the transpose runs on torch's current stream, the library's copy
+            # on its own: finish the transpose before handing over the pointer
+            torch.cuda.current_stream(Cc.device).synchronize()
             where = DEVICE
         else:
             Cc = _host_f64(C, "F")
