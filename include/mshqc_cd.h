@@ -58,7 +58,13 @@ enum mshqc_cd_precision {
                              one power-of-two scale, integer hi/lo carried in
                              FP16, three products per pair, exact FP32
                              accumulation on the tensor cores; FP64
-                             denominators, diagonal integrals and energies  */
+                             denominators, diagonal integrals and energies;
+                             the half transforms and the backward's
+                             transposed transforms as FP64 products of
+                             int8 slices (5 x 7 bits per operand row) on
+                             the tensor cores, about 2^-32 of the row
+                             maxima per term (MSHQC_CD_TRANSFORM=f64 in the
+                             environment: FP64 DMMA instead)             */
 };
 
 enum mshqc_cd_kind {
@@ -153,7 +159,8 @@ MSHQC_CD_API int mshqc_cd_set_orbitals(mshqc_cd_ctx* ctx, int spin, const double
  * CholeskyUMP2::transform_cholesky_vectors (src/mp2/cholesky_ump2.cc:244-293)
  * and CholeskyOMP2::transform_vectors (src/mp2/cholesky_omp2.cc:71-92).
  * B_out (o*v*M, see header) may be NULL to keep the result on the device
- * only. */
+ * only.  MSHQC_CD_FP64 returns FP64 DMMA products; MSHQC_CD_FP16X3 may
+ * return the int8-slice products (or reuse FP64 ones already computed). */
 MSHQC_CD_API int mshqc_cd_transform(mshqc_cd_ctx* ctx, int spin, int precision,
                        double* B_out, int where);
 /* MP2 correlation energy.  Replaces the pair loop of CholeskyRMP2::compute
