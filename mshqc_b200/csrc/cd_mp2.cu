@@ -754,7 +754,8 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
         const size_t pp = sizeof(double) * (size_t)(o * N);
         const int64_t nq_max = std::max<int64_t>(1, (int64_t)(2 * kSliceBytes / (pa + pb + pp)));
         const int64_t qc = vectors_chunk_size(ctx);
-        const int64_t nq = std::min(nq_max, qc);
+        // (batches are the z dimension of the transposed-slicing grid)
+        const int64_t nq = std::min<int64_t>(std::min(nq_max, qc), 65535);
         CD_ALLOC(ctx->oz_a, pa * nq, false);
         CD_ALLOC(ctx->oz_b, pb * nq, false);
         CD_ALLOC(ctx->oz_p, pp * nq, false);
