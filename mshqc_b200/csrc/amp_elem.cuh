@@ -58,6 +58,12 @@ struct AmpElemArgs {
     double* prow;           // [ox * oy][rsx] sum_b r per pair and row a (or null)
     double* pcol;           // [ox * oy][ksy] sum_a r per pair and column b (or null)
     double* pocc;           // [ox * oy] sum_ab r per pair (or null)
+    // nchunk > 1: each pair's row tiles are split over nchunk CTAs (CTA
+    // lp * nchunk + c takes chunk c of local pair lp = ii * nbj + jj); their
+    // column sums, energies and totals go to cpcol [lp][c][ksy], cpart and
+    // cpocc [lp][c], and amp_chunks_combine_kernel adds the chunks in order
+    int nchunk;
+    double* cpcol; double* cpart; double* cpocc;
 };
 
 namespace amp_detail {
@@ -87,7 +93,7 @@ __device__ __forceinline__ void store_hilo8(const double* t, uint16_t* hi, uint1
 }  // namespace amp_detail
 
 template <int MODE, bool SPLIT>
-__global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
+__global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
     using TS = typename std::conditional<SPLIT, float, double>::type;
     constexpr bool kW = MODE != AMP_OPPOSITE_SPIN;   // (ib|ja) needed
     __shared__ TS Vt[32][33];
@@ -97,13 +103,18 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
     __shared__ double red_e[8], red_r[8];
     const TS* S = static_cast<const TS*>(p.S);
     const int ta = p.rsx / 32, tb = p.ksy / 32;
-    const int ii = (int)(blockIdx.x / p.nbj), jj = (int)(blockIdx.x % p.nbj);
+    const int R = p.nchunk > 1 ? p.nchunk : 1;
+    const int lp = (int)(blockIdx.x / R), ch = (int)(blockIdx.x % R);
+    const int ii = lp / p.nbj, jj = lp % p.nbj;
+    const int xb0 = ch * ta / R, xb1 = (ch + 1) * ta / R;   // this CTA's row tiles
     const int i = p.i0 + ii, j = p.j0 + jj;
     const long long pair = (long long)i * p.oy + j;          // over all occupied rows
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
     const double eij = p.eox[i] + p.eoy[j];
     double* prow = p.prow ? p.prow + pair * p.rsx : nullptr;
-    double* pcol = p.pcol ? p.pcol + pair * p.ksy : nullptr;
+    double* pcol = !p.pcol ? nullptr
+                   : R == 1 ? p.pcol + pair * p.ksy
+                            : p.cpcol + ((long long)lp * R + ch) * p.ksy;
     const TS* Srow = S + (long long)ii * p.rsx * p.ldS + (long long)jj * p.csy;
     // this thread's four elements of tile (a0, b0): rows ty + 8k, column tx
     // (V); the transposed tile (b0, a0) for W
@@ -116,12 +127,12 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
         }
     };
     TS vn[4], wn[4];
-    load_tile(0, 0, vn, wn);
+    if (xb0 < xb1) load_tile(xb0 * 32, 0, vn, wn);
     double esum = 0.0, rtot = 0.0;
     // row blocks outer, column blocks inner: a thread's rows stay fixed over
     // the inner loop, so their sums over b stay in registers; the column sums
     // of a tile are reduced across the warps and added to pcol in xb order
-    for (int xb = 0; xb < ta; ++xb) {
+    for (int xb = xb0; xb < xb1; ++xb) {
         const int a0 = xb * 32;
         double rsum[4] = {0.0, 0.0, 0.0, 0.0};
         for (int yb = 0; yb < tb; ++yb) {
@@ -134,7 +145,7 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
             // the next tile's loads overlap this tile's arithmetic and stores
             if (yb + 1 < tb)
                 load_tile(a0, b0 + 32, vn, wn);
-            else if (xb + 1 < ta)
+            else if (xb + 1 < xb1)
                 load_tile(a0 + 32, 0, vn, wn);
             __syncthreads();
             double cp = 0.0;
@@ -199,7 +210,7 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
                 double c = 0.0;
 #pragma unroll
                 for (int w = 0; w < 8; ++w) c += colpart[w][tx];
-                pcol[b0 + tx] = (xb == 0 ? 0.0 : pcol[b0 + tx]) + p.wgt * c;
+                pcol[b0 + tx] = (xb == xb0 ? 0.0 : pcol[b0 + tx]) + p.wgt * c;
             }
             __syncthreads();   // Vt, Wt, T, colpart are refilled by the next tile
         }
@@ -229,8 +240,38 @@ __global__ void __launch_bounds__(256) amp_elem_kernel(AmpElemArgs p) {
             e += red_e[w];
             r += red_r[w];
         }
-        p.partial[pair] = p.wgt * e;
-        if (p.pocc) p.pocc[pair] = p.wgt * r;
+        if (R == 1) {
+            p.partial[pair] = p.wgt * e;
+            if (p.pocc) p.pocc[pair] = p.wgt * r;
+        } else {
+            p.cpart[(long long)lp * R + ch] = p.wgt * e;
+            if (p.pocc) p.cpocc[(long long)lp * R + ch] = p.wgt * r;
+        }
+    }
+}
+
+// The chunk partials of amp_elem_kernel (nchunk > 1) of the nbi x nbj local
+// pairs added in chunk order into the per-pair outputs: one thread per
+// (local pair, column b); the b == 0 thread also does energy and total.
+static __global__ void amp_chunks_combine_kernel(AmpElemArgs p, int npl) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)npl * p.ksy) return;
+    const int lp = (int)(idx / p.ksy), b = (int)(idx % p.ksy);
+    const int R = p.nchunk;
+    const long long pair = (long long)(p.i0 + lp / p.nbj) * p.oy + p.j0 + lp % p.nbj;
+    if (p.pcol) {
+        double sc = 0.0;
+        for (int c = 0; c < R; ++c) sc += p.cpcol[((long long)lp * R + c) * p.ksy + b];
+        p.pcol[pair * p.ksy + b] = sc;
+    }
+    if (b == 0) {
+        double e = 0.0, r = 0.0;
+        for (int c = 0; c < R; ++c) {
+            e += p.cpart[(long long)lp * R + c];
+            if (p.pocc) r += p.cpocc[(long long)lp * R + c];
+        }
+        p.partial[pair] = e;
+        if (p.pocc) p.pocc[pair] = r;
     }
 }
 

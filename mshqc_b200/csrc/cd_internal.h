@@ -93,6 +93,7 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf amp2;          // backward: second half of the staging (lo)
     mshqc_cd::DevBuf ampT, ampT2;   // backward: transposed opposite-spin amplitudes (hi, lo)
     mshqc_cd::DevBuf dsum;          // backward: per-pair row / column / total sums for dE/de
+    mshqc_cd::DevBuf amp_chunks;    // backward: per-chunk column sums, energies, totals of split pairs
     mshqc_cd::DevBuf W;             // backward: integral staging / C_vir-contracted Gamma
     mshqc_cd::DevBuf grad[4];       // backward: dC / deps per spin
     mshqc_cd::DevBuf diag_os;       // sum_Q B_alpha[i][a] B_beta[i][a] (opposite-spin diagonal)
@@ -147,6 +148,7 @@ struct mshqc_cd_ctx {
         ampT.release();
         ampT2.release();
         dsum.release();
+        amp_chunks.release();
         W.release();
         for (auto& s : spin) {
             s.C.release();

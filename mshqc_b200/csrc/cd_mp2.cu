@@ -1045,11 +1045,29 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             }
             e.partial = partial;
             e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
+            // split each pair's row tiles over several CTAs when the block
+            // pair alone does not fill the GPU several times over
+            const int ta = (int)(dx.VR / 32), npl = (int)(nI * nJ);
+            int nch = 1;
+            while (nch < 4 && 2 * nch <= ta && (int64_t)npl * nch < 8LL * ctx->num_sms) nch *= 2;
+            e.nchunk = nch;
+            if (nch > 1) {
+                const size_t per = (size_t)npl * nch;
+                CD_ALLOC(ctx->amp_chunks, sizeof(double) * per * ((size_t)dy.VR + 2), false);
+                e.cpcol = ctx->amp_chunks.as<double>();
+                e.cpart = e.cpcol + per * dy.VR;
+                e.cpocc = e.cpart + per;
+            }
             begin_stage(ctx, ST_AMP_ELEM);
-            amp_elem_kernel<MODE, true><<<(unsigned)(nI * nJ), 256, 0, ctx->stream>>>(e);
-            end_stage(ctx);
+            amp_elem_kernel<MODE, true><<<(unsigned)(npl * nch), 256, 0, ctx->stream>>>(e);
             CD_CUDA(cudaGetLastError());
             ctx->launches++;
+            if (nch > 1) {
+                amp_chunks_combine_kernel<<<(unsigned)cdiv((int64_t)npl * dy.VR, 256), 256, 0, ctx->stream>>>(e, npl);
+                CD_CUDA(cudaGetLastError());
+                ctx->launches++;
+            }
+            end_stage(ctx);
             // Gamma_sx[I] += A x B_sy[J]  (K range of J inside the transposed B of spin sy)
             // first K chunk of block J (I) inside a 256-row block of BT
             const size_t kJ = (size_t)J0 * dy.VR / 16 * 4096, kI = (size_t)I0 * dx.VR / 16 * 4096;
