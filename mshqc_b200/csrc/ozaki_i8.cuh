@@ -13,7 +13,8 @@
 //   2^{e_x + e_y} sum_{w=0}^{S-1} 2^{-7(w+2)} sum_{s+t=w} (d^x_s . d^y_t),
 // keeping the S(S+1)/2 slice pairs with s + t < S.  Each slice product is an
 // exact 32-bit integer tensor-core accumulation (|sum| <= S 127^2 K < 2^31
-// for K <= 26624) and the S weights are combined in FP64 in the epilogue.
+// for K <= 26624); the epilogue combines the S weighted sums exactly in 64-bit
+// integers and rounds once to FP64.
 // With S = 5 the error per term is below about 2^-32 (2^e_x 2^e_y): far
 // below the fixed-point splitting that follows on the mixed path, which is
 // the only path that uses these products (the FP64 path keeps FP64 FMAs).
