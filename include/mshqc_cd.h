@@ -103,6 +103,16 @@ MSHQC_CD_API const char* mshqc_cd_last_error(void);
 MSHQC_CD_API int mshqc_cd_abi_version(void);
 /* Run on a caller stream (cudaStream_t) instead of the context's own. */
 MSHQC_CD_API int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream);
+/* Share one gradient among nranks contexts, one per GPU (no counterpart in
+ * the reference, which runs on one node): mshqc_cd_mp2_gradient of this
+ * context then computes the units k of its backward (block pairs of occupied
+ * orbitals; occupied blocks on the FP64 path) with k % nranks == rank and
+ * returns that share's energy, dE/dC and dE/deps.  Their sums over the ranks
+ * (one all-reduce of 3 + 2 N^2 + 2 N doubles at most) are the full result.
+ * The half transforms and the transposed transforms run in full on every
+ * rank; mshqc_cd_mp2_energy and the OMP2 entry points are not partitioned.
+ * (0, 1) is the default: everything on this context. */
+MSHQC_CD_API int mshqc_cd_set_partition(mshqc_cd_ctx* ctx, int rank, int nranks);
 /* Bytes of device memory the context holds. */
 MSHQC_CD_API int mshqc_cd_device_bytes(mshqc_cd_ctx* ctx, int64_t* bytes);
 /* Number of kernels this context has launched so far. */

@@ -65,6 +65,7 @@ SIGNATURES = {
     "mshqc_cd_last_error": (ctypes.c_char_p, []),
     "mshqc_cd_abi_version": (_i32, []),
     "mshqc_cd_set_stream": (_i32, [_vp, _vp]),
+    "mshqc_cd_set_partition": (_i32, [_vp, _i32, _i32]),
     "mshqc_cd_device_bytes": (_i32, [_vp, ctypes.POINTER(_i64)]),
     "mshqc_cd_launch_count": (_i32, [_vp, ctypes.POINTER(_i64)]),
     "mshqc_cd_stage_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
@@ -173,6 +174,12 @@ class Context:
 
     def set_stream(self, stream_handle: int | None):
         _check(self._lib.mshqc_cd_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def set_partition(self, rank: int, nranks: int):
+        """Compute only share `rank` of `nranks` of the gradient's backward
+        (sum the shares' energies and derivatives over the ranks)."""
+        _check(self._lib.mshqc_cd_set_partition(self._h, int(rank), int(nranks)))
+        return self
 
     def device_bytes(self) -> int:
         b = ctypes.c_int64(0)

@@ -301,6 +301,15 @@ int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream) {
     return MSHQC_CD_OK;
 }
 
+int mshqc_cd_set_partition(mshqc_cd_ctx* ctx, int rank, int nranks) {
+    CD_CHECK_CTX();
+    if (nranks < 1 || rank < 0 || rank >= nranks)
+        return set_error(MSHQC_CD_ERR_ARG, "partition needs 0 <= rank < nranks");
+    ctx->part_rank = rank;
+    ctx->part_size = nranks;
+    return MSHQC_CD_OK;
+}
+
 int mshqc_cd_stage_times(mshqc_cd_ctx* ctx, double* ms_out, int n_out) {
     CD_CHECK_CTX();
     if (!ms_out || n_out < 0) return set_error(MSHQC_CD_ERR_ARG, "bad output");

@@ -108,6 +108,12 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf oz_p;          // per-batch FP64 partial products (transposed transforms)
     bool diag_os_valid = false;
     int fixed_point_exact = 1;      // Cauchy-Schwarz bound of the last tensor-core pass held
+    // share of the backward computed by this context (mshqc_cd_set_partition):
+    // units (block pairs, or occupied blocks of the FP64 passes) k with
+    // k % part_size == part_rank, counted from 0 in every gradient call
+    int part_rank = 0, part_size = 1;
+    bool part_active = false;
+    int64_t part_next = 0;
 
     std::vector<double> pair_energy[3];  // host copies, row-major [i][j]
 

@@ -36,6 +36,13 @@ __global__ void sum_partials_kernel(const double* __restrict__ parts, int S, int
     out[k] = alpha * acc;
 }
 
+// Partitioned backward: whether the next unit (block pair, or occupied block
+// of an FP64 pass) belongs to this context's share.
+bool owns_next(mshqc_cd_ctx* ctx) {
+    const int64_t k = ctx->part_next++;
+    return !ctx->part_active || ctx->part_size <= 1 || k % ctx->part_size == ctx->part_rank;
+}
+
 int require_inputs(mshqc_cd_ctx* ctx, int spin) {
     if (!ctx->L_set) return set_error(MSHQC_CD_ERR_STATE, "Cholesky vectors not set");
     if (!ctx->spin[spin].set)
@@ -810,14 +817,16 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
     const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 4, size_t(16) << 30));
     const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(budget / per_i)));
     CD_ALLOC(ctx->amp, per_i * bi, false);
-    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, false);
+    // zeroed: with a partition the blocks of other ranks stay zero
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, ctx->part_active);
     CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
     const int64_t units_per_i = (int64_t)o * nb * nb;
-    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), false);
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), ctx->part_active);
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
     const size_t smem = pair_f64_detail::SMEM_BYTES;
     CD_CUDA(cudaFuncSetAttribute(amp_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int i0 = 0; i0 < o; i0 += bi) {
+        if (!owns_next(ctx)) continue;
         const int nbi = (int)std::min<int64_t>(bi, o - i0);
         AmpF64Args a{};
         a.X = s.B64.as<double>();
@@ -1006,6 +1015,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
     for (int64_t I0 = 0; I0 < dx.o; I0 += bI) {
         const int nI = (int)std::min<int64_t>(bI, dx.o - I0);
         for (int64_t J0 = kSym ? I0 : 0; J0 < dy.o; J0 += bJ) {
+            if (!owns_next(ctx)) continue;
             const int nJ = (int)std::min<int64_t>(bJ, dy.o - J0);
             const bool mirror = !kSym || J0 != I0;
             VtileArgs a{};
@@ -1102,11 +1112,13 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
     CD_ALLOC(ctx->W, per_i / 2 * bi, false);
     CD_ALLOC(ctx->amp, per_i / 2 * bi, false);
     const int64_t npairs = dx.o * dy.o;
-    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.vp + dy.vp + 1)), false);
+    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.vp + dy.vp + 1)), ctx->part_active);
+    if (ctx->part_active) CD_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * (size_t)npairs, ctx->stream));
     double* prow = ctx->dsum.as<double>();
     double* pcol = prow + npairs * dx.vp;
     double* pocc = pcol + npairs * dy.vp;
     for (int i0 = 0; i0 < dx.o; i0 += bi) {
+        if (!owns_next(ctx)) continue;
         const int nbi = (int)std::min<int64_t>(bi, dx.o - i0);
         const double* Xb = X.B64.as<double>() + (int64_t)i0 * dx.vp * Mp;
         // S[(i,a)][(j,b)] = sum_Q X[(i,a)][Q] Y[(j,b)][Q]
@@ -1258,6 +1270,12 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
     CD_RC(require_inputs(ctx, 0));
     if (unres) CD_RC(require_inputs(ctx, 1));
     const int64_t N = ctx->N;
+    // the partition applies to this call's backward only
+    struct PartitionScope {
+        mshqc_cd_ctx* c;
+        explicit PartitionScope(mshqc_cd_ctx* x) : c(x) { c->part_active = c->part_size > 1; c->part_next = 0; }
+        ~PartitionScope() { c->part_active = false; }
+    } part_scope(ctx);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     reset_stages(ctx);
     CD_CUDA(cudaEventRecord(e0, ctx->stream));
