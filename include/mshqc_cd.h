@@ -105,12 +105,18 @@ MSHQC_CD_API int mshqc_cd_abi_version(void);
 MSHQC_CD_API int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream);
 /* Share one gradient among nranks contexts, one per GPU (no counterpart in
  * the reference, which runs on one node): mshqc_cd_mp2_gradient of this
- * context then computes the units k of its backward (block pairs of occupied
- * orbitals; occupied blocks on the FP64 path) with k % nranks == rank and
- * returns that share's energy, dE/dC and dE/deps.  Their sums over the ranks
- * (one all-reduce of 3 + 2 N^2 + 2 N doubles at most) are the full result.
- * The half transforms and the transposed transforms run in full on every
- * rank; mshqc_cd_mp2_energy and the OMP2 entry points are not partitioned.
+ * context then computes its share of the backward's units (block pairs of
+ * occupied orbitals; occupied blocks on the FP64 path) and returns that
+ * share's energy, dE/dC and dE/deps.  Their sums over the ranks (one
+ * all-reduce of 3 + 2 N^2 + 2 N doubles at most) are the full result.
+ * The shares: with nranks > 1 the occupied block sizes depend only on the
+ * orbital counts, the number of vectors and nranks (never on the free device
+ * memory, which differs between GPUs), giving about 32 block pairs per rank;
+ * each unit is weighed by its integral-tile and Gamma work and the units are
+ * dealt out longest first to the least-loaded rank.  All ranks compute the
+ * same plan, so every unit is computed exactly once.  The half transforms
+ * and the transposed transforms run in full on every rank;
+ * mshqc_cd_mp2_energy and the OMP2 entry points are not partitioned.
  * (0, 1) is the default: everything on this context. */
 MSHQC_CD_API int mshqc_cd_set_partition(mshqc_cd_ctx* ctx, int rank, int nranks);
 /* Bytes of device memory the context holds. */
@@ -275,9 +281,10 @@ MSHQC_CD_API int mshqc_cd_omp2(mshqc_cd_ctx* ctx, const mshqc_cd_omp2_config* cf
  *         returns once its kernels are queued; synchronize the stream before
  *         reading energy.
  *
- * Set-up happens on the first call with each device current (it looks up the
- * scratch address and the kernel attributes): make that first call outside
- * any stream capture.  No scratch word needs to start at zero: a call writes
+ * Set-up happens on the first call with each device current, and again on
+ * the first call in a new CUDA context of that device (after cudaDeviceReset):
+ * it looks up the scratch address and the kernel attributes.  Make that first
+ * call outside any stream capture.  No scratch word needs to start at zero: a call writes
  * all the scratch it reads before reading it.  All calls on one device share
  * the scratch, so calls that overlap in time (different streams or host
  * threads) race on it: order them (one stream, or events).  Inputs are not

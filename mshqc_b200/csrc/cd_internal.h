@@ -109,11 +109,14 @@ struct mshqc_cd_ctx {
     bool diag_os_valid = false;
     int fixed_point_exact = 1;      // Cauchy-Schwarz bound of the last tensor-core pass held
     // share of the backward computed by this context (mshqc_cd_set_partition):
-    // units (block pairs, or occupied blocks of the FP64 passes) k with
-    // k % part_size == part_rank, counted from 0 in every gradient call
+    // the units (block pairs, or occupied blocks of the FP64 passes) of a
+    // gradient call are numbered from 0 in the order the passes visit them;
+    // part_owned[k] says whether unit k is this rank's (a cost-balanced plan
+    // that every rank computes alike, see plan_partition in cd_mp2.cu)
     int part_rank = 0, part_size = 1;
     bool part_active = false;
     int64_t part_next = 0;
+    std::vector<uint8_t> part_owned;
 
     std::vector<double> pair_energy[3];  // host copies, row-major [i][j]
 

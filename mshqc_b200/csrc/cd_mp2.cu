@@ -37,10 +37,67 @@ __global__ void sum_partials_kernel(const double* __restrict__ parts, int S, int
 }
 
 // Partitioned backward: whether the next unit (block pair, or occupied block
-// of an FP64 pass) belongs to this context's share.
+// of an FP64 pass) belongs to this context's share.  Units beyond the plan
+// (which a mismatch between plan_partition and the passes would produce)
+// belong to nobody; run_gradient checks the count afterwards.
 bool owns_next(mshqc_cd_ctx* ctx) {
     const int64_t k = ctx->part_next++;
-    return !ctx->part_active || ctx->part_size <= 1 || k % ctx->part_size == ctx->part_rank;
+    if (!ctx->part_active) return true;
+    return k < (int64_t)ctx->part_owned.size() && ctx->part_owned[(size_t)k] != 0;
+}
+
+// ---------------------------------------------------------------------------
+// occupied block sizes of the backward passes
+// ---------------------------------------------------------------------------
+// Unpartitioned, a block is as large as a share of the free device memory
+// allows (fewer, larger launches).  Partitioned, the block sizes are a
+// function of the problem dimensions and the number of ranks only, so that
+// every rank enumerates the same units whatever memory its GPU has free: at
+// most the staging these fixed budgets hold, and small enough that there are
+// about 32 units per rank for the cost-balanced plan (or 4 per rank for the
+// FP64 passes, whose units are blocks of rows).  MSHQC_CD_BWD_BLOCK (occupied
+// orbitals per block) overrides both rules in every pass.
+constexpr size_t kPartTcBudget = size_t(16) << 30;
+constexpr size_t kPartF64Budget = size_t(4) << 30;
+
+int64_t env_block() {
+    const char* env = std::getenv("MSHQC_CD_BWD_BLOCK");
+    if (!env) return 0;
+    const long long b = std::atoll(env);
+    return b > 0 ? (int64_t)b : 0;
+}
+
+// block sizes (rows bI, columns bJ) of a tensor-core pass; staging per (i, j)
+// of S (FP32, VS columns) and the four BF16 amplitude operands
+void tc_block_sizes(const mshqc_cd_ctx* ctx, int64_t ox, int64_t oy, int64_t VRx, int64_t VRy, int64_t VSy,
+                    bool sym, size_t free_budget, int64_t* bI, int64_t* bJ) {
+    const bool part = ctx->part_active;
+    const size_t budget = part ? kPartTcBudget : free_budget;
+    if (sym) {
+        const double per_b2 = (double)VRx * (4.0 * VSy + 8.0 * VRy);
+        *bI = std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)std::sqrt((double)budget / per_b2)));
+        if (part) {
+            // nb blocks give nb (nb + 1) / 2 block pairs: about 32 per rank
+            const int64_t nb = (int64_t)std::ceil(std::sqrt(64.0 * ctx->part_size));
+            *bI = std::min<int64_t>(*bI, std::max<int64_t>(1, cdiv(ox, nb)));
+        }
+    } else {
+        const double per_i = (double)VRx * oy * (4.0 * VSy + 8.0 * VRy);
+        *bI = std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)((double)budget / per_i)));
+        if (part) *bI = std::min<int64_t>(*bI, std::max<int64_t>(1, cdiv(ox, 4 * (int64_t)ctx->part_size)));
+    }
+    if (const int64_t b = env_block()) *bI = std::min<int64_t>(ox, b);
+    *bJ = sym ? *bI : oy;
+}
+
+// rows per block of an FP64 pass with per_i staging bytes per occupied row
+int64_t f64_block_rows(const mshqc_cd_ctx* ctx, int64_t ox, size_t per_i, size_t free_budget, size_t part_budget) {
+    const bool part = ctx->part_active;
+    const size_t budget = std::max<size_t>(per_i, part ? part_budget : free_budget);
+    int64_t bi = std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)(budget / per_i)));
+    if (part) bi = std::min<int64_t>(bi, std::max<int64_t>(1, cdiv(ox, 4 * (int64_t)ctx->part_size)));
+    if (const int64_t b = env_block()) bi = std::min<int64_t>(ox, b);
+    return bi;
 }
 
 int require_inputs(mshqc_cd_ctx* ctx, int spin) {
@@ -814,8 +871,8 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t per_i = sizeof(double) * (size_t)vp * o * vp;
-    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 4, size_t(16) << 30));
-    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(budget / per_i)));
+    const int bi = (int)f64_block_rows(ctx, o, per_i, std::min<size_t>(free_b / 4, size_t(16) << 30),
+                                       kPartF64Budget);
     CD_ALLOC(ctx->amp, per_i * bi, false);
     // zeroed: with a partition the blocks of other ranks stay zero
     CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, ctx->part_active);
@@ -982,22 +1039,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
     const size_t budget = std::min<size_t>((free_b + held) / 3, size_t(40) << 30);
     // block sizes: rows bI, columns bJ (all of them for the opposite spin)
     int64_t bI, bJ;
-    if (kSym) {
-        const double per_b2 = (double)dx.VR * (4.0 * dy.VS + 8.0 * dy.VR);   // S + A1 + A2 per (i, j)
-        bI = bJ = std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)std::sqrt((double)budget / per_b2)));
-    } else {
-        const double per_i = (double)dx.VR * dy.o * (4.0 * dy.VS + 8.0 * dy.VR);
-        bI = std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)((double)budget / per_i)));
-        bJ = dy.o;
-    }
-    // MSHQC_CD_BWD_BLOCK (occupied orbitals per block) overrides the choice
-    if (const char* env = std::getenv("MSHQC_CD_BWD_BLOCK")) {
-        const long long b = std::atoll(env);
-        if (b > 0) {
-            bI = std::min<int64_t>(dx.o, b);
-            if (kSym) bJ = bI;
-        }
-    }
+    tc_block_sizes(ctx, dx.o, dy.o, dx.VR, dy.VR, dy.VS, kSym, budget, &bI, &bJ);
     const size_t n_amp = sizeof(uint16_t) * (size_t)(bI * dx.VR) * (size_t)(bJ * dy.VR);
     CD_ALLOC(ctx->amp, n_amp, false);
     CD_ALLOC(ctx->amp2, n_amp, false);
@@ -1107,8 +1149,8 @@ int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double*
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t per_i = 2 * sizeof(double) * (size_t)dx.vp * ldS;
-    const size_t budget = std::max<size_t>(per_i, std::min<size_t>(free_b / 4, size_t(32) << 30));
-    const int bi = (int)std::max<int64_t>(1, std::min<int64_t>(dx.o, (int64_t)(budget / per_i)));
+    const int bi = (int)f64_block_rows(ctx, dx.o, per_i, std::min<size_t>(free_b / 4, size_t(32) << 30),
+                                       2 * kPartF64Budget);
     CD_ALLOC(ctx->W, per_i / 2 * bi, false);
     CD_ALLOC(ctx->amp, per_i / 2 * bi, false);
     const int64_t npairs = dx.o * dy.o;
@@ -1260,6 +1302,65 @@ int gradient_unrestricted(mshqc_cd_ctx* ctx, int precision, double* const dC[2],
     return MSHQC_CD_OK;
 }
 
+// The shares of a partitioned gradient call.  Enumerates the backward's units
+// in the order the passes visit them, with the partitioned block sizes (a
+// function of the dimensions and the rank count only), weighs each by its
+// tensor-core or DMMA work (integral tiles + Gamma products, in (i, j) pair
+// units: a diagonal block pair has no mirrored Gamma product), and deals them
+// out longest first to the least-loaded rank (ties to the lower rank).  Every
+// rank computes the same plan and keeps its own units.
+int plan_partition(mshqc_cd_ctx* ctx, int kind, int precision) {
+    std::vector<double> cost;
+    const bool unres = kind == MSHQC_CD_UNRESTRICTED;
+    auto tc_pass = [&](int sx, int sy, bool sym) {
+        const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
+        int64_t bI, bJ;
+        tc_block_sizes(ctx, dx.o, dy.o, dx.VR, dy.VR, dy.VS, sym, 0, &bI, &bJ);
+        for (int64_t I0 = 0; I0 < dx.o; I0 += bI) {
+            const int64_t nI = std::min(bI, dx.o - I0);
+            for (int64_t J0 = sym ? I0 : 0; J0 < dy.o; J0 += bJ) {
+                const int64_t nJ = std::min(bJ, dy.o - J0);
+                const bool mirror = !sym || J0 != I0;
+                cost.push_back((double)nI * nJ * (mirror ? 3.0 : 2.0));
+            }
+        }
+    };
+    auto f64_pass = [&](int sx, int sy, bool os) {
+        const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
+        const size_t per_i = 2 * sizeof(double) * (size_t)dx.vp * (size_t)(dy.o * dy.vp);
+        const int64_t bi = f64_block_rows(ctx, dx.o, per_i, 0, 2 * kPartF64Budget);
+        for (int64_t i0 = 0; i0 < dx.o; i0 += bi)
+            cost.push_back((double)std::min(bi, dx.o - i0) * dy.o * (os ? 3.0 : 2.0));
+    };
+    if (!unres && precision == MSHQC_CD_FP64) {
+        const BwdDims d = bwd_dims(ctx, 0);
+        const size_t per_i = sizeof(double) * (size_t)d.vp * d.o * d.vp;
+        const int64_t bi = f64_block_rows(ctx, d.o, per_i, 0, kPartF64Budget);
+        for (int64_t i0 = 0; i0 < d.o; i0 += bi) cost.push_back((double)std::min(bi, d.o - i0));
+    } else if (!unres) {
+        tc_pass(0, 0, true);
+    } else if (precision == MSHQC_CD_FP16X3) {
+        tc_pass(0, 0, true);
+        tc_pass(1, 1, true);
+        tc_pass(0, 1, false);
+    } else {
+        f64_pass(0, 0, false);
+        f64_pass(1, 1, false);
+        f64_pass(0, 1, true);
+    }
+    std::vector<size_t> order(cost.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+    std::vector<double> load((size_t)ctx->part_size, 0.0);
+    ctx->part_owned.assign(cost.size(), 0);
+    for (size_t k : order) {
+        const size_t r = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[r] += cost[k];
+        if ((int)r == ctx->part_rank) ctx->part_owned[k] = 1;
+    }
+    return MSHQC_CD_OK;
+}
+
 }  // namespace
 
 int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out, double* dC_a,
@@ -1282,6 +1383,7 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
     CD_RC(ensure_transform(ctx, 0, precision));
     if (unres) CD_RC(ensure_transform(ctx, 1, precision));
     CD_CUDA(cudaEventRecord(e1, ctx->stream));
+    if (ctx->part_active) CD_RC(plan_partition(ctx, kind, precision));
     double* dC[2] = {nullptr, nullptr};
     double* de[2] = {nullptr, nullptr};
     for (int s = 0; s < (unres ? 2 : 1); ++s) {
@@ -1300,6 +1402,9 @@ int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_
     } else {
         CD_RC(gradient_restricted_tc(ctx, dC[0], de[0], &energy));
     }
+    if (ctx->part_active && ctx->part_next != (int64_t)ctx->part_owned.size())
+        return set_error(MSHQC_CD_ERR_STATE, "partition plan covers " + std::to_string(ctx->part_owned.size()) +
+                                                 " units, the backward visited " + std::to_string(ctx->part_next));
     CD_CUDA(cudaEventRecord(e2, ctx->stream));
     CD_CUDA(cudaEventSynchronize(e2));
     collect_stages(ctx);

@@ -31,6 +31,35 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratch
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_setup_ctx[kMaxDevices] = {};   // context of the cached set-up (0: none)
+
+// Unique id of the calling thread's current CUDA context (never reused within
+// a process, so a context made after cudaDeviceReset has a new one), through
+// the driver entry points the runtime hands out; 0 when unavailable.
+unsigned long long current_context_id() {
+    using GetCurrentFn = int (*)(void**);
+    using GetIdFn = int (*)(void*, unsigned long long*);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrentFn>(f1);
+            get_id = reinterpret_cast<GetIdFn>(f2);
+        }
+        looked_up = true;
+    }
+    if (!get_current || !get_id) return 0;
+    void* c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != 0 || !c || get_id(c, &id) != 0) return 0;
+    return id;
+}
 
 // (i, j), i <= j, row by row; and (x, y), x <= y, row by row -- the unit order
 // of the context path's tables.
@@ -47,11 +76,15 @@ static __global__ void noalloc_tables_kernel(int o, int nb, int2* __restrict__ p
     }
 }
 
-// Once per device, with that device current: the address of the scratch
-// array and the kernel's shared-memory limit.
+// Once per device and CUDA context, with that device current: the address of
+// the scratch array and the kernel's shared-memory limit.  Both belong to the
+// context, so a new context on the device (after cudaDeviceReset) sets up
+// again; without the context id the set-up runs on every call (it allocates
+// nothing either way).
 int noalloc_setup(int dev, void** out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_ptr[dev]) {
+    const unsigned long long ctx_id = current_context_id();
+    if (g_scratch_ptr[dev] && ctx_id != 0 && g_setup_ctx[dev] == ctx_id) {
         *out = g_scratch_ptr[dev];
         return MSHQC_CD_OK;
     }
@@ -71,6 +104,7 @@ int noalloc_setup(int dev, void** out) {
                              (int)pair_f64_detail::SMEM_BYTES);
     if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(pair kernel)");
     g_scratch_ptr[dev] = p;
+    g_setup_ctx[dev] = ctx_id;
     *out = p;
     return MSHQC_CD_OK;
 }

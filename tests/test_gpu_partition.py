@@ -3,8 +3,10 @@ after another on one GPU: the shares' energies and derivatives add up to the
 unpartitioned gradient (FP64 path: to rounding, 1e-12 of the largest entry;
 mixed path: 1e-8, since its transposed transforms slice each share's Gamma
 with its own row scales, ~2^-32 relative per term), restricted and
-unrestricted, with small occupied blocks so that there are many block pairs
-to share.  A share that owns no unit returns zeros."""
+unrestricted.  With a partition the block sizes come from the dimensions and
+the rank count alone (about 32 block pairs per rank), so every share gets
+work (a nonzero energy) and the shares do not change when a GPU has less
+free memory."""
 import numpy as np
 import pytest
 
@@ -31,23 +33,17 @@ def close(x, y, tol):
     return np.max(np.abs(x - y)) <= tol * np.max(np.abs(y))
 
 
-@pytest.mark.parametrize("unres", [False, True])
-@pytest.mark.parametrize("precision", [capi.FP16X3, capi.FP64])
-@pytest.mark.parametrize("nranks", [2, 3])
-def test_shares_add_up(monkeypatch, unres, precision, nranks):
-    monkeypatch.setenv("MSHQC_CD_BWD_BLOCK", "3")
-    inp = twin(110, 11, 260, seed=17, nocc_beta=9 if unres else None)
-    kind = capi.UNRESTRICTED if unres else capi.RESTRICTED
-    with capi.Context(0) as ctx:
+def shares_of(ctx, inp, unres, kind, precision, nranks):
+    out = []
+    for r in range(nranks):
+        ctx.set_partition(r, nranks)
         setup(ctx, inp, unres)
-        full = ctx.mp2_gradient(kind, precision)
-        shares = []
-        for r in range(nranks):
-            ctx.set_partition(r, nranks)
-            setup(ctx, inp, unres)
-            shares.append(ctx.mp2_gradient(kind, precision))
-        ctx.set_partition(0, 1)
-        again = ctx.mp2_gradient(kind, precision)      # back to the whole gradient
+        out.append(ctx.mp2_gradient(kind, precision))
+    ctx.set_partition(0, 1)
+    return out
+
+
+def check_sum(shares, full, unres, precision):
     tot = lambda f: sum(f(g) for g in shares)
     tol = 1e-12 if precision == capi.FP64 else 1e-8
     for k in ("ss_aa", "ss_bb", "os", "total"):
@@ -57,7 +53,66 @@ def test_shares_add_up(monkeypatch, unres, precision, nranks):
     if unres:
         assert close(tot(lambda g: g.dC_b), full.dC_b, tol)
         assert close(tot(lambda g: g.deps_b), full.deps_b, tol)
+
+
+@pytest.mark.parametrize("unres", [False, True])
+@pytest.mark.parametrize("precision", [capi.FP16X3, capi.FP64])
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_shares_add_up(monkeypatch, unres, precision, nranks):
+    monkeypatch.delenv("MSHQC_CD_BWD_BLOCK", raising=False)
+    inp = twin(110, 13, 260, seed=17, nocc_beta=11 if unres else None)
+    kind = capi.UNRESTRICTED if unres else capi.RESTRICTED
+    with capi.Context(0) as ctx:
+        setup(ctx, inp, unres)
+        full = ctx.mp2_gradient(kind, precision)
+        shares = shares_of(ctx, inp, unres, kind, precision, nranks)
+        again = ctx.mp2_gradient(kind, precision)      # back to the whole gradient
+    check_sum(shares, full, unres, precision)
+    # every rank got units (13 occupied orbitals give at least 4 per rank)
+    for g in shares:
+        assert g.energy["total"] != 0.0
+        assert np.max(np.abs(g.dC_a)) > 0.0
     assert abs(again.energy["total"] - full.energy["total"]) <= 1e-12 * abs(full.energy["total"])
+
+
+@pytest.mark.parametrize("precision", [capi.FP16X3, capi.FP64])
+def test_block_override_applies_to_every_pass(monkeypatch, precision):
+    """MSHQC_CD_BWD_BLOCK sets the occupied block of the FP64 passes too: with
+    blocks of 2 of 9 orbitals every one of 3 ranks owns units."""
+    monkeypatch.setenv("MSHQC_CD_BWD_BLOCK", "2")
+    inp = twin(90, 9, 200, seed=5, nocc_beta=8)
+    with capi.Context(0) as ctx:
+        for unres in (False, True):
+            kind = capi.UNRESTRICTED if unres else capi.RESTRICTED
+            setup(ctx, inp, unres)
+            full = ctx.mp2_gradient(kind, precision)
+            shares = shares_of(ctx, inp, unres, kind, precision, 3)
+            check_sum(shares, full, unres, precision)
+            assert all(g.energy["total"] != 0.0 for g in shares)
+
+
+def test_shares_do_not_depend_on_free_memory(monkeypatch):
+    """The shares are the same when the GPU has most of its memory taken by
+    another allocation (a rank on a busier GPU) as when it is free: at this
+    size an unpartitioned call would pick smaller blocks with 4 GB free."""
+    import torch
+    monkeypatch.delenv("MSHQC_CD_BWD_BLOCK", raising=False)
+    inp = twin(400, 40, 1600, seed=23)
+    with capi.Context(0) as ctx:
+        setup(ctx, inp, False)
+        free_run = shares_of(ctx, inp, False, capi.RESTRICTED, capi.FP16X3, 2)
+    free_b, _ = torch.cuda.mem_get_info(0)
+    ballast = torch.empty(max(0, free_b - (4 << 30)), dtype=torch.uint8, device="cuda:0")
+    try:
+        with capi.Context(0) as ctx:
+            setup(ctx, inp, False)
+            busy_run = shares_of(ctx, inp, False, capi.RESTRICTED, capi.FP16X3, 2)
+    finally:
+        del ballast
+        torch.cuda.empty_cache()
+    for a, b in zip(free_run, busy_run):
+        assert a.energy["total"] == b.energy["total"]
+        assert np.array_equal(a.dC_a, b.dC_a)
 
 
 def test_partition_arguments_are_checked():
