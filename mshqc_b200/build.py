@@ -20,6 +20,9 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmshqc_cuda.so")
 
 CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_omp2.cu", "cd_vectors.cu", "cd_decompose.cu", "cd_noalloc.cu"]
+# host-only C++ (the AO integral engine), compiled by g++ with OpenMP
+HOST_SOURCES = ["ao_integrals.cc"]
+HOST_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-fopenmp", "-march=x86-64-v3"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -61,6 +64,7 @@ def build_cuda(verbose: bool = False, force: bool = False, extra_flags=()) -> st
     os.makedirs(LIBDIR, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
     deps.append(os.path.join(ROOT, "include", "mshqc_cd.h"))
+    deps.append(os.path.join(ROOT, "include", "mshqc_ao.h"))
     if not force and not _stale(LIB, deps):
         return LIB
     objdir = os.path.join(LIBDIR, "obj")
@@ -71,9 +75,14 @@ def build_cuda(verbose: bool = False, force: bool = False, extra_flags=()) -> st
         _run([nvcc(), *_host_compiler_flags(), *NVCC_FLAGS, *extra_flags, "-c",
               os.path.join(CSRC, src), "-o", obj], verbose)
         objs.append(obj)
+    gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+    for src in HOST_SOURCES:
+        obj = os.path.join(objdir, src.replace(".cc", ".o"))
+        _run([gxx, *HOST_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj], verbose)
+        objs.append(obj)
     tmp = LIB + ".tmp"
     _run([nvcc(), *_host_compiler_flags(), "-gencode", "arch=compute_100a,code=sm_100a",
-          "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-cudart", "static"], verbose)
+          "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-cudart", "static", "-lgomp"], verbose)
     os.replace(tmp, LIB)
     return LIB
 

@@ -44,6 +44,8 @@ def _load():
         lib.ref_omp2.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, i, i, _dp, d, i, d, d, i,
                                  _dp, _ip, _dp, _dp]
         lib.ref_cholesky_decompose.argtypes = [i, _dp, d, i, _dp, _ip]
+        lib.ref_omp2_mp2_part.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, i, i, i, _dp]
+        lib.ref_rhf_cdrmp2.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, d, i, _dp, _dp, _dp, _ip]
         _lib = lib
     return _lib
 
@@ -123,6 +125,40 @@ def omp2_pieces(L, Ca, Cb, ea, eb, na, nb, H, nthreads=0):
                                _p(Gvvb), _p(Fa), _p(Fb), _p(wa), _p(wb)))
     return dict(e_mp2=e[0], seconds=e[1], Goo_a=Gooa, Gvv_a=Gvva, Goo_b=Goob,
                 Gvv_b=Gvvb, F_a=Fa, F_b=Fb, w_a=wa, w_b=wb)
+
+
+def rhf_cdrmp2(Z, xyz, S, T, V, eri, chol_thr=1e-6, e_thr=1e-12, d_thr=1e-10, nthreads=0):
+    """The reference's RHF (src/scf/rhf.cc) and CholeskyRMP2 constructor 1
+    (decomposes the ERI tensor itself, src/mp2/cholesky_rmp2.cc:20-41) on the
+    given AO integrals; atoms Z, xyz (bohr).  Returns dict(e_scf, e_corr,
+    n_vectors, iterations, converged, C (N, N), eps (N,), nocc)."""
+    lib = _load()
+    N = S.shape[0]
+    Zc, X = _c(Z), _c(np.asarray(xyz).reshape(-1))
+    S, T, V = _f(S), _f(T), _f(V)
+    E = _c(np.asarray(eri).reshape(-1))
+    out = np.zeros(5)
+    C = np.zeros((N, N), order="F")
+    eps = np.zeros(N)
+    nocc = ctypes.c_int(0)
+    _check(lib.ref_rhf_cdrmp2(N, len(Zc), _p(Zc), _p(X), _p(S), _p(T), _p(V), _p(E), chol_thr, e_thr, d_thr,
+                              nthreads, _p(out), _p(C), _p(eps), ctypes.byref(nocc)))
+    return dict(e_scf=out[0], e_corr=out[1], n_vectors=int(out[2]), iterations=int(out[3]),
+                converged=bool(out[4]), C=C, eps=eps, nocc=nocc.value)
+
+
+def omp2_mp2_part(L, Ca, Cb, ea, eb, na, nb, nthreads=0):
+    """The MP2 part of one OMP2 gradient evaluation (transforms, t2, E, OPDM of
+    both spins), timed inside the reference: dict(e_mp2, seconds)."""
+    lib = _load()
+    L = _c(L)
+    M = L.shape[0]
+    N = Ca.shape[0]
+    Ca, Cb = _f(Ca), _f(Cb)
+    ea, eb = _c(ea), _c(eb)
+    out = np.zeros(2)
+    _check(lib.ref_omp2_mp2_part(N, M, _p(L), _p(Ca), _p(Cb), _p(ea), _p(eb), na, nb, nthreads, _p(out)))
+    return dict(e_mp2=out[0], seconds=out[1])
 
 
 def omp2(L, Ca, Cb, ea, eb, na, nb, H, e_scf=0.0, max_iter=50, e_thr=1e-6,

@@ -48,6 +48,7 @@
 namespace mshqc {
 namespace oracle_stub {
 extern Eigen::MatrixXd g_core_hamiltonian;
+extern Eigen::MatrixXd g_overlap, g_kinetic, g_nuclear;
 extern Eigen::Tensor<double, 4> g_eri;
 extern bool g_have_eri;
 }  // namespace oracle_stub
@@ -249,6 +250,39 @@ int ref_omp2_pieces(int N, int M, const double* L, const double* Ca,
     }
 }
 
+// The MP2 part of one CholeskyOMP2 gradient evaluation, as compute() runs it
+// (src/mp2/cholesky_omp2.cc:445-449): both spins' half transforms and t2
+// (compute_t2_amplitudes :94-183), the energy from t2 (:189-230) and the
+// OPDM blocks of both spins (:232-326); the generalized Fock builds that
+// follow are not timed.  out[0] = E_mp2, out[1] = seconds.
+int ref_omp2_mp2_part(int N, int M, const double* L, const double* Ca, const double* Cb,
+                      const double* ea, const double* eb, int na, int nb, int nthreads,
+                      double* out) {
+    try {
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+        Quiet q(true);
+        Molecule mol;
+        BasisSet basis = make_basis(N);
+        auto ints = std::make_shared<IntegralEngine>(mol, basis);
+        integrals::CholeskyERI chol(1e-6);
+        fill_cholesky(chol, N, M, L);
+        SCFResult scf = make_scf(N, Ca, Cb, ea, eb, na, nb, 0.0);
+        CholeskyOMP2Config cfg;
+        cfg.print_level = 0;
+        CholeskyOMP2 omp2(mol, basis, ints, scf, cfg, chol);
+        auto t0 = std::chrono::steady_clock::now();
+        omp2.compute_t2_amplitudes();
+        out[0] = omp2.compute_mp2_energy_from_t2();
+        omp2.build_opdm_alpha();
+        omp2.build_opdm_beta();
+        out[1] = seconds_since(t0);
+        return 0;
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        return -1;
+    }
+}
+
 // Full CholeskyOMP2::compute() (src/mp2/cholesky_omp2.cc:427-512).
 // out[0..2] = energy_mp2_corr, energy_total, energy_scf; out[3] = seconds;
 // iters[0] = iterations, iters[1] = converged.  Final C_alpha/C_beta are
@@ -286,6 +320,61 @@ int ref_omp2(int N, int M, const double* L, const double* Ca, const double* Cb,
         return 0;
     } catch (const std::exception& ex) {
         g_err = ex.what();
+        return -1;
+    }
+}
+
+// The reference's closed-shell pipeline on given AO integrals: RHF
+// (src/scf/rhf.cc, DIIS src/scf/diis.cc) on S, T, V and the ERI tensor
+// (N^4, element (ij|kl) at ((i N + j) N + k) N + l), then CholeskyRMP2 with
+// constructor 1 (src/mp2/cholesky_rmp2.cc:20-41: decomposes the ERI tensor
+// from the engine with cholesky_threshold) and compute().  Atoms: Z[natom],
+// xyz[3 natom] in bohr.  out[0] = E_SCF (total), out[1] = E_corr,
+// out[2] = number of Cholesky vectors, out[3] = SCF iterations,
+// out[4] = converged; C_out (N*N column-major), eps_out (N), and nocc_out.
+int ref_rhf_cdrmp2(int N, int natom, const double* Z, const double* xyz, const double* S, const double* T,
+                   const double* V, const double* eri, double chol_thr, double e_thr, double d_thr, int nthreads,
+                   double* out, double* C_out, double* eps_out, int* nocc_out) {
+    try {
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+        Quiet q(true);
+        oracle_stub::g_core_hamiltonian.resize(0, 0);
+        oracle_stub::g_overlap = Eigen::Map<const Eigen::MatrixXd>(S, N, N);
+        oracle_stub::g_kinetic = Eigen::Map<const Eigen::MatrixXd>(T, N, N);
+        oracle_stub::g_nuclear = Eigen::Map<const Eigen::MatrixXd>(V, N, N);
+        oracle_stub::g_eri = Eigen::Tensor<double, 4>(N, N, N, N);
+        std::memcpy(oracle_stub::g_eri.data(), eri, sizeof(double) * (size_t)N * N * N * N);
+        oracle_stub::g_have_eri = true;
+        Molecule mol;
+        for (int a = 0; a < natom; ++a)
+            mol.add_atom((int)std::lround(Z[a]), xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]);
+        BasisSet basis = make_basis(N);
+        auto ints = std::make_shared<IntegralEngine>(mol, basis);
+        SCFConfig scfg;
+        scfg.print_level = 0;
+        scfg.max_iterations = 200;
+        scfg.energy_threshold = e_thr;
+        scfg.density_threshold = d_thr;
+        RHF rhf(mol, basis, ints, scfg);
+        SCFResult r = rhf.compute();
+        CholeskyRMP2Config cfg;
+        cfg.cholesky_threshold = chol_thr;
+        cfg.print_level = 0;
+        CholeskyRMP2 rmp2(mol, basis, ints, r, cfg);
+        auto res = rmp2.compute();
+        out[0] = r.energy_total;
+        out[1] = res.e_corr;
+        out[2] = rmp2.cholesky_ptr_->n_vectors();
+        out[3] = r.iterations;
+        out[4] = r.converged ? 1.0 : 0.0;
+        std::memcpy(C_out, r.C_alpha.data(), sizeof(double) * (size_t)N * N);
+        std::memcpy(eps_out, r.orbital_energies_alpha.data(), sizeof(double) * (size_t)N);
+        *nocc_out = r.n_occ_alpha;
+        oracle_stub::g_have_eri = false;
+        return 0;
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        oracle_stub::g_have_eri = false;
         return -1;
     }
 }
