@@ -11,17 +11,28 @@ recipe (mshqc_b200/synthetic.py) at the scaled magnitude |E_corr| ~ 0.05 o Eh.
 Its FP64 AO vectors would take 256 GB, so the library generates them on the
 device chunk by chunk (mshqc_cd_gen_vectors) wherever they are read.
 
-One step = AO->MO half transform + integral tiles + amplitude pass + Gamma
-GEMM + transposed transforms, i.e. one mp2_gradient call, in the mixed
-precision (scaled FP16x3 on the tensor cores).  The FP64 path is timed once on
-the same inputs for the mixed-vs-FP64 comparison and the energy / gradient
-errors.
+One step = one mp2_gradient call in the mixed precision: AO->MO half
+transform, integral tiles of the unique pairs (the energy comes out of them),
+element-wise amplitude pass, Gamma GEMM, transposed transforms.  The FP64
+path is timed once on the same inputs for the mixed-vs-FP64 comparison and
+the energy / gradient errors.
 
-`value` = FP64-equivalent algorithmic TFLOP/s over all ranks with the inputs
-resident in HBM (work 2 F_T + 2 F_E + 2 v^2 M o^2; F_T = 2 M N o (N+v),
-F_E = v^2 M o (o+1)); `e2e` = the same metric through the C ABI from host
-buffers, copies inside the timed region.  Multi-GPU runs are replicas
-(independent inputs per rank, weak scaling, no data-path collective).
+`value` = FP64-equivalent algorithmic TFLOP/s of the work the step performs
+(split products not counted), over all ranks, inputs resident in HBM:
+F_T + F_E + F_G + F_Tt with F_T = 2 M N o (N + v) (half transform),
+F_E = v^2 M o (o + 1) (integral tiles of the unique pairs i <= j),
+F_G = 2 v^2 M o^2 (Gamma), F_Tt = 2 M N o (N + 2 v) (transposed transforms);
+an energy-only step is F_T + F_E.  `e2e` = the same metric through the C ABI
+from host buffers, copies inside the timed region.  With --gpus N > 1 the
+ranks share one gradient (mshqc_cd_set_partition, NCCL all-reduce of the
+shares); --parallelism replicas runs N independent copies instead.
+
+The reference arm (--impl reference) runs the reference's own CPU code
+(oracle/_ref, compiled from its sources) on a bounded sample of the workload:
+the same synthetic recipe at the same ratios v/o and M/N with fewer occupied
+orbitals, timed inside the reference, and extrapolated to the workload as
+o^5 (the operation count of the reference's loops at fixed ratios) from the
+sample's own rate; same-size workloads that fit (N <= 400) run in full.
 """
 from __future__ import annotations
 
@@ -65,10 +76,18 @@ DEFAULT_WORKLOAD = "cdmp2_grad_n2000_o200_m8000"
 # algorithmic work (FP64-equivalent flops; split products not counted)
 # ---------------------------------------------------------------------------
 def flops_transform(N, o, M):
+    """AO->MO half transform of one spin: 2 M N o (N + v)."""
     return 2.0 * M * N * o * (N + (N - o))
 
 
+def flops_transposed(N, o, M):
+    """dE/dC of one spin from Gamma: dC_vir (2 M N o v), W = Gamma C_vir^T
+    (2 M N o v), dC_occ (2 M N^2 o)."""
+    return 2.0 * M * N * o * (N + 2 * (N - o))
+
+
 def flops_energy(N, o, M):
+    """(ia|jb) of the unique pairs i <= j: 2 v^2 M o (o + 1) / 2."""
     v = N - o
     return 1.0 * v * v * M * o * (o + 1)
 
@@ -78,28 +97,27 @@ def flops_gamma(N, o, M):
     return 2.0 * v * v * M * o * o
 
 
-def workload_flops(N, o, M, gradient):
-    if not gradient:
-        return flops_transform(N, o, M) + flops_energy(N, o, M)
-    return 2 * flops_transform(N, o, M) + 2 * flops_energy(N, o, M) + flops_gamma(N, o, M)
-
-
-def unrestricted_parts(N, oa, ob, M):
-    """(transforms, integral tiles, Gamma) of the unrestricted energy +
-    gradient: both spins transformed forward and back; the backward forms
-    every same-spin (unique pairs i <= j) and opposite-spin (ia|jb) once and
-    Gamma_alpha, Gamma_beta (two products for the opposite-spin block)."""
-    va, vb = N - oa, N - ob
-    tr = 2 * (flops_transform(N, oa, M) + flops_transform(N, ob, M))
-    tiles = 2.0 * M * (va * va * oa * (oa + 1) / 2 + vb * vb * ob * (ob + 1) / 2 + va * vb * oa * ob)
-    gam = 2.0 * M * (va * va * oa * oa + vb * vb * ob * ob + 2.0 * va * vb * oa * ob)
-    return tr, tiles, gam
+def workload_parts(w):
+    """{stage: flops} of the work one step performs."""
+    N, o, M = w["N"], w["o"], w["M"]
+    if w.get("kind") == "unrestricted":
+        ob = w["ob"]
+        va, vb = N - o, N - ob
+        tiles = 2.0 * M * (va * va * o * (o + 1) / 2 + vb * vb * ob * (ob + 1) / 2 + va * vb * o * ob)
+        parts = {"transform": flops_transform(N, o, M) + flops_transform(N, ob, M), "tiles": tiles}
+        if w["gradient"]:
+            parts["gamma"] = 2.0 * M * (va * va * o * o + vb * vb * ob * ob + 2.0 * va * vb * o * ob)
+            parts["transposed"] = flops_transposed(N, o, M) + flops_transposed(N, ob, M)
+        return parts
+    parts = {"transform": flops_transform(N, o, M), "tiles": flops_energy(N, o, M)}
+    if w["gradient"]:
+        parts["gamma"] = flops_gamma(N, o, M)
+        parts["transposed"] = flops_transposed(N, o, M)
+    return parts
 
 
 def workload_flops_w(w):
-    if w.get("kind") == "unrestricted":
-        return sum(unrestricted_parts(w["N"], w["o"], w["ob"], w["M"]))
-    return workload_flops(w["N"], w["o"], w["M"], w["gradient"])
+    return sum(workload_parts(w).values())
 
 
 # ---------------------------------------------------------------------------
@@ -207,40 +225,78 @@ def measure_fp64_peak(torch, device):
 # ---------------------------------------------------------------------------
 # reference CPU path (oracle/_ref: the reference's own code, compiled here)
 # ---------------------------------------------------------------------------
-REF_SAMPLE = dict(N=300, o=10, M=1200)
+REF_FULL_MAX_N = 400        # workloads up to this size run in full on the CPU
+REF_SAMPLE_O = 12           # occupied orbitals of a scaled sample
+REF_CALIBRATION_O = (8, 12, 16)
 
 
-def run_reference_once(w, seed, nthreads):
-    """One bounded sample of the workload on the reference's own CPU code:
-    CholeskyOMP2's energy + orbital-gradient evaluation (t2, E, OPDM,
-    generalized Fock, w_ai; src/mp2/cholesky_omp2.cc:441-466) for gradient
-    workloads (separate alpha / beta orbitals for the unrestricted one),
-    CholeskyRMP2::compute for energy workloads."""
+def sample_shape(w, o_s):
+    """The workload's shape scaled to o_s occupied orbitals at its own ratios
+    v/o and M/N (the beta count keeps its offset from alpha)."""
+    N, o, M = w["N"], w["o"], w["M"]
+    if o_s >= o:
+        return N, o, w.get("ob", o), M
+    N_s = max(o_s + 2, int(round(N * o_s / o)))
+    M_s = max(4, int(round(M * N_s / N)))
+    ob_s = max(1, o_s - (o - w.get("ob", o)))
+    return N_s, o_s, ob_s, M_s
+
+
+def run_reference_sample(w, o_s, seed, nthreads):
+    """The reference's own CPU code on the workload scaled to o_s occupied
+    orbitals (in full when o_s >= o): CholeskyOMP2's MP2 part of one gradient
+    evaluation (both spins' transforms and t2, the energy, the OPDM blocks;
+    src/mp2/cholesky_omp2.cc:445-449) for gradient workloads, with separate
+    beta orbitals for the unrestricted one, CholeskyRMP2::compute for energy
+    workloads.  Returns (seconds inside the reference, description)."""
     from mshqc_b200 import synthetic as syn
     from oracle import ref
-    N, o, M = REF_SAMPLE["N"], REF_SAMPLE["o"], REF_SAMPLE["M"]
+    N, o, ob, M = sample_shape(w, o_s)
     unres = w.get("kind") == "unrestricted"
-    ob = o - 1 if unres else o
     base = syn.make_inputs(N, o, M, seed=seed)
     sig = syn.twin_sigma(N, o, M, base.alpha.eps)
     inp = syn.make_inputs(N, o, M, seed=seed, sigma=sig, nocc_beta=ob if unres else None)
     a = inp.alpha
     b = inp.beta if unres else a
     if w["gradient"]:
-        H = np.eye(N)   # the cost of the Fock build does not depend on H
-        r = ref.omp2_pieces(inp.L, a.C, b.C, a.eps, b.eps, o, ob, H, nthreads=nthreads)
-        what = "CholeskyOMP2 energy + w_ai"
+        r = ref.omp2_mp2_part(inp.L, a.C, b.C, a.eps, b.eps, o, ob, nthreads=nthreads)
+        what = "CholeskyOMP2 t2 + energy + OPDM"
     else:
         r = ref.rmp2(inp.L, a.C, a.eps, o, nthreads=nthreads)
         what = "CholeskyRMP2::compute"
-    if unres:
-        flops = sum(unrestricted_parts(N, o, ob, M))
-    else:
-        flops = workload_flops(N, o, M, w["gradient"])
-    return r["seconds"], flops, f"N={N}, o={o}{'/%d' % ob if unres else ''}, M={M} {what}"
+    shape = f"N={N}, o={o}{'/%d' % ob if unres else ''}, M={M}"
+    return r["seconds"], f"{what} at {shape}"
+
+
+def ref_extrapolation(w, o_s):
+    """Factor from the sample's time to the workload's: (o / o_s)^5."""
+    return (w["o"] / float(o_s)) ** 5
+
+
+def calibrate_reference(w, nthreads, seed=7):
+    """Times of the reference on samples of the workload at REF_CALIBRATION_O
+    occupied orbitals and the slope of log t against log o (reported; the
+    extrapolation itself uses o^5 from the sample's own rate)."""
+    ts = []
+    for o_s in REF_CALIBRATION_O:
+        t, _ = run_reference_sample(w, o_s, seed, nthreads)
+        ts.append(t)
+    x = np.log(np.asarray(REF_CALIBRATION_O, dtype=float))
+    y = np.log(np.asarray(ts))
+    slope = float(np.polyfit(x, y, 1)[0])
+    return ts, slope
+
+
+def reference_plan(w):
+    """(o of the sample, whether the sample is the whole workload)."""
+    if w["N"] <= REF_FULL_MAX_N:
+        return w["o"], True
+    return REF_SAMPLE_O, False
 
 
 def bench_reference(args, w, rank, world):
+    """The reference arm: rank 0 alone times the reference's CPU path on all
+    host cores; the other ranks exit without work."""
     if rank != 0:
         return
     from oracle import ref
@@ -248,35 +304,74 @@ def bench_reference(args, w, rank, world):
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmshqc_ref.so not built"}))
         return
+    flops = workload_flops_w(w)
+    o_s, full = reference_plan(w)
+    calib = None
+    if not full:
+        calib = calibrate_reference(w, nthreads)
     for s in range(args.warmup):
-        run_reference_once(w, s, nthreads)
-    times, flops, sample = [], 0.0, ""
+        run_reference_sample(w, o_s, s, nthreads)
+    times, sample = [], ""
     for s in range(args.steps):
-        t, f, sample = run_reference_once(w, 100 + s, nthreads)
+        t, sample = run_reference_sample(w, o_s, 100 + s, nthreads)
         times.append(t)
-        flops = f
-    tot = sum(times)
-    value = flops * args.steps / tot / 1e12
+    t_sample = sum(times) / len(times)
+    t_step = t_sample if full else t_sample * ref_extrapolation(w, o_s)
+    value = flops / t_step / 1e12
+    note = ("the workload itself" if full else
+            f"{sample}, extrapolated to the workload as (o/{o_s})^5 from the sample's rate; "
+            f"calibration o={list(REF_CALIBRATION_O)}: {[round(float(t), 3) for t in calib[0]]} s, "
+            f"measured slope {calib[1]:.2f}")
+    cpu = {"value": value, "unit": "TFLOP/s", "cores": nthreads, "kind": "reference",
+           "sample": sample if full else note, "sample_seconds": t_sample,
+           "extrapolated": not full}
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": sample},
-        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": nthreads,
-                         "kind": "reference", "sample": sample},
-        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
+        "ms_per_step": 1e3 * t_step, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded recipe, scaled twin)",
+        "config": {"workload": args.workload, "same_config": full,
+                   "sample": sample if full else note},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def cpu_baseline_line(w):
+    """cpu_baseline of the GPU arm: the calibration samples of the reference
+    (about 10-30 s of CPU work), extrapolated like the reference arm."""
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "error": "oracle/_ref/libmshqc_ref.so not built"}
+    nthreads = os.cpu_count() or 1
+    flops = workload_flops_w(w)
+    o_s, full = reference_plan(w)
+    if full:
+        t, sample = run_reference_sample(w, o_s, 7, nthreads)
+        return {"value": flops / t / 1e12, "unit": "TFLOP/s", "cores": nthreads, "kind": "reference",
+                "sample": sample, "seconds": t, "extrapolated": False}
+    ts, slope = calibrate_reference(w, nthreads)
+    t_step = ts[REF_CALIBRATION_O.index(REF_SAMPLE_O)] * ref_extrapolation(w, REF_SAMPLE_O)
+    N_s, _, ob_s, M_s = sample_shape(w, REF_SAMPLE_O)
+    return {"value": flops / t_step / 1e12, "unit": "TFLOP/s", "cores": nthreads, "kind": "reference",
+            "sample": (f"reference at o={list(REF_CALIBRATION_O)} (ratios of the workload), "
+                       f"{[round(float(t), 3) for t in ts]} s, slope {slope:.2f}; "
+                       f"o={REF_SAMPLE_O} (N={N_s}, M={M_s}) extrapolated as (o/{REF_SAMPLE_O})^5"),
+            "seconds": sum(ts), "extrapolated_step_s": t_step, "extrapolated": True}
 
 
 # ---------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------
+STAGE_KEYS = ("transform", "split", "pair_energy", "amplitude", "gamma", "transposed", "other", "amp_elem")
+
+
 def bench_gpu(args, w, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from mshqc_b200 import capi
+    from mshqc_b200 import shard
     from mshqc_b200 import synthetic as syn
 
     torch.cuda.set_device(local_rank)
@@ -287,7 +382,9 @@ def bench_gpu(args, w, rank, world, local_rank):
     unres = w.get("kind") == "unrestricted"
     kind = capi.UNRESTRICTED if unres else capi.RESTRICTED
     ob = w.get("ob", o)
-    seed = 1000 + rank
+    shared = world > 1 and args.parallelism == "shared" and gradient
+    # shared: every rank holds the same inputs; replicas: independent ones
+    seed = 1000 + (0 if shared else rank)
 
     orb = syn.make_orbitals(N, o, seed)
     orb_b = syn.make_orbitals(N, ob, seed + 7919) if unres else orb
@@ -306,12 +403,18 @@ def bench_gpu(args, w, rank, world, local_rank):
         ctx.gen_vectors(N, M, seed, sigma)
     else:
         ctx.set_vectors(L_dev)
+    if shared:
+        ctx.set_partition(rank, world)
 
     def step(context, precision, C, eps):
         context.set_orbitals(capi.ALPHA, C, eps, o)            # new orbitals: full recompute
         if unres:
             context.set_orbitals(capi.BETA, Cb_dev, eb_dev, ob)
         if gradient:
+            if shared:
+                g = context.mp2_gradient_torch(kind, precision, device=dev)
+                torch.cuda.current_stream(dev).synchronize()
+                return shard.allreduce_gradient(g)
             return context.mp2_gradient(kind, precision)
         return context.mp2_energy(kind, precision)
 
@@ -348,9 +451,15 @@ def bench_gpu(args, w, rank, world, local_rank):
     exact = ctx.mixed_exact() if prec != capi.FP64 else True
 
     elapsed = max_over_ranks(elapsed, dev)
-    flops = workload_flops_w(w)
-    value = world * flops * args.steps / elapsed / 1e12
+    parts = workload_parts(w)
+    flops = sum(parts.values())
+    jobs = 1 if shared else world
+    value = jobs * flops * args.steps / elapsed / 1e12
     mixed_res = r
+    st = {k: statistics.median(s[k] for s in stages) for k in stages[0]}
+
+    def host(x):
+        return x.detach().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x)
 
     # ---- FP64 path on the same inputs (comparison and error) ---------------
     fp64 = {}
@@ -358,29 +467,33 @@ def bench_gpu(args, w, rank, world, local_rank):
         # one FP64 step, not warmed up: the same transforms ran above and the
         # FP64 kernels' first-launch cost is negligible next to the step
         torch.cuda.synchronize()
+        barrier()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         r64 = step(ctx, capi.FP64, C_dev, e_dev)
         t1.record(stream)
         torch.cuda.synchronize()
-        ms64 = t0.elapsed_time(t1)
+        ms64 = max_over_ranks(t0.elapsed_time(t1), dev)
+        st64 = ctx.stage_times()
+        dgemm = measure_fp64_peak(torch, dev)
+        fp64 = {"fp64_ms_per_step": ms64, "fp64_tflops": jobs * flops / (ms64 / 1e3) / 1e12,
+                "fp64_stage_ms": st64, "fp64_dgemm_tflops": dgemm,
+                "fp64_frac_of_dgemm": (flops / (ms64 / 1e3) / 1e12) / dgemm,
+                "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps)}
         if gradient:
             e3, e64 = mixed_res.energy["total"], r64.energy["total"]
-            pairs = [(mixed_res.dC_a, r64.dC_a, mixed_res.deps_a, r64.deps_a)]
+            pairs = [(host(mixed_res.dC_a), host(r64.dC_a), host(mixed_res.deps_a), host(r64.deps_a))]
             if unres:
-                pairs.append((mixed_res.dC_b, r64.dC_b, mixed_res.deps_b, r64.deps_b))
-            fp64 = {"fp64_ms_per_step": ms64, "fp64_tflops": flops / (ms64 / 1e3) / 1e12,
-                    "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps),
-                    "energy_fp64": e64, "energy_mixed": e3,
-                    "energy_error_uEh": abs(e3 - e64) * 1e6,
-                    "max_abs_dC_error": max(float(np.max(np.abs(x - y))) for x, y, _, _ in pairs),
-                    "max_abs_deps_error": max(float(np.max(np.abs(x - y))) for _, _, x, y in pairs),
-                    "max_abs_dC": max(float(np.max(np.abs(y))) for _, y, _, _ in pairs)}
+                pairs.append((host(mixed_res.dC_b), host(r64.dC_b), host(mixed_res.deps_b), host(r64.deps_b)))
+            fp64.update({"energy_fp64": e64, "energy_mixed": e3,
+                         "energy_error_uEh": abs(e3 - e64) * 1e6,
+                         "max_abs_dC_error": max(float(np.max(np.abs(x - y))) for x, y, _, _ in pairs),
+                         "max_abs_deps_error": max(float(np.max(np.abs(x - y))) for _, _, x, y in pairs),
+                         "max_abs_dC": max(float(np.max(np.abs(y))) for _, y, _, _ in pairs)})
         else:
-            fp64 = {"fp64_ms_per_step": ms64,
-                    "speedup_mixed_vs_fp64": ms64 / (1e3 * elapsed / args.steps),
-                    "energy_error_uEh": abs(mixed_res["total"] - r64["total"]) * 1e6}
+            fp64.update({"energy_fp64": r64["total"], "energy_mixed": mixed_res["total"],
+                         "energy_error_uEh": abs(mixed_res["total"] - r64["total"]) * 1e6})
 
     # ---- end to end through the C ABI from pinned host buffers ------------
     e2e = None
@@ -397,6 +510,8 @@ def bench_gpu(args, w, rank, world, local_rank):
         torch.cuda.empty_cache()
         ctx_h = capi.Context(local_rank)
         ctx_h.set_stream(stream.cuda_stream)
+        if shared:
+            ctx_h.set_partition(rank, world)
         L_np = None if gen else L_host.numpy()
 
         def step_e2e():
@@ -408,7 +523,8 @@ def bench_gpu(args, w, rank, world, local_rank):
             if unres:
                 ctx_h.set_orbitals(capi.BETA, Cb_host, eb_host, ob)
             if gradient:
-                return ctx_h.mp2_gradient(kind, prec)       # results copied to host
+                g = ctx_h.mp2_gradient(kind, prec)       # results copied to host
+                return shard.allreduce_gradient(g, device=dev) if shared else g
             return ctx_h.mp2_energy(kind, prec)
 
         step_e2e()
@@ -423,7 +539,7 @@ def bench_gpu(args, w, rank, world, local_rank):
         nspin = 2 if unres else 1
         h2d = (0 if gen else L_np.nbytes) + nspin * (C_host.nbytes + e_host.nbytes)
         d2h = 8 * 7 + (nspin * (N * N + N) * 8 if gradient else 0)
-        e2e = {"value": world * flops * args.steps / e2e_elapsed / 1e12, "unit": "TFLOP/s",
+        e2e = {"value": jobs * flops * args.steps / e2e_elapsed / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": 1e3 * e2e_elapsed / args.steps}
         ctx_h.close()
@@ -432,17 +548,14 @@ def bench_gpu(args, w, rank, world, local_rank):
 
     # ---- roofline of the dominant kernel ----------------------------------
     peaks, peak_src = measured_peaks()
-    st = {k: statistics.median(s[k] for s in stages) for k in stages[0]}
-    if gradient and unres:
-        _, ftiles, fgam = unrestricted_parts(N, o, ob, M)
-        cand = {"amplitude": ("vtile_tc_kernel", ftiles), "gamma": ("gamma_tc_kernel", fgam)}
-    elif gradient:
-        cand = {"amplitude": ("vtile_tc_kernel", flops_energy(N, o, M)),   # unique pairs i <= j
-                "gamma": ("gamma_tc_kernel", flops_gamma(N, o, M))}
+    if gradient:
+        cand = {"amplitude": ("vtile_tc_kernel", parts["tiles"]), "gamma": ("gamma_tc_kernel", parts["gamma"])}
     else:
-        cand = {"pair_energy": ("pair_energy_tc_kernel<RESTRICTED>", flops_energy(N, o, M))}
+        cand = {"pair_energy": ("pair_energy_tc_kernel", parts["tiles"])}
     dom = max(cand, key=lambda k: st.get(k, 0.0))
     kname, kflops = cand[dom]
+    if shared:
+        kflops /= world                     # this rank's share of the units
     kms = st[dom]
     achieved = kflops / (kms / 1e3) / 1e12 if kms > 0 else None
     if prec == capi.FP64:
@@ -452,47 +565,51 @@ def bench_gpu(args, w, rank, world, local_rank):
         peak = peaks["bf16_tflops_sustained"] / 3.0
         peak_note = (f"dense 16-bit tensor peak ({peak_src}, sustained "
                      f"{peaks['bf16_tflops_sustained']}) / 3: three products per useful product")
+    traffic = roofline_traffic(kname, w)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if shared else "weak", "vs_baseline": None,
             "dtype": ("f64" if prec == capi.FP64 else
-                      "fp16x3 (scaled fixed point, exact f32 accumulate; f64 denominators, sums)"),
+                      "fp16x3 (integer hi/lo fixed point on the tensor cores, f32 accumulate; bf16x3 Gamma; "
+                      "int8-slice transforms; f64 denominators and sums)"),
             "data": "synthetic (seeded recipe, scaled twin, device Philox stream for L)",
             "config": {"workload": args.workload, "N": N, "o": o, "v": N - o, "M": M,
                        **({"o_beta": ob} if unres else {}),
                        "kind": "unrestricted" if unres else "restricted",
                        "precision": w["precision"], "gradient": gradient,
-                       "sigma": sigma, "parallelism": f"replicas{world}",
+                       "sigma": sigma,
+                       "parallelism": (f"shared{world}" if shared else f"replicas{world}"),
                        "vectors": "generated on the device per chunk" if gen else "stored",
                        "l2": "inputs larger than L2 (AO vectors %.1f GB%s, MO vectors %.2f GB)" % (
                            N * N * M * 8 / 1e9, ", regenerated, never stored" if gen else "",
                            o * (N - o) * M * 8 / 1e9),
+                       "work_tflop": {k: v / 1e12 for k, v in parts.items()},
                        "stage_ms": st, "mixed_exact_accumulation": exact, **fp64},
             "clocks": clk,
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": None,
-                         "traffic_note": "not captured at this size; small-case DRAM traffic does not scale "
-                                         "in proportion (profiles/launches_cdmp2_grad_n2000_o200_m8000.md)",
+                         "traffic": traffic.get("bytes") if traffic else None,
+                         "traffic_note": traffic.get("note") if traffic else "no capture for this kernel",
                          "peak_source": peak_note, "kernel_ms_per_step": kms},
         }
         if not args.no_cpu_baseline:
             try:
-                from oracle import ref
-                if ref.available():
-                    nthreads = os.cpu_count() or 1
-                    ts, fs, sample = run_reference_once(w, 7, nthreads)
-                    line["cpu_baseline"] = {"value": fs / ts / 1e12, "unit": "TFLOP/s",
-                                            "cores": nthreads, "kind": "reference",
-                                            "sample": sample, "seconds": ts}
+                line["cpu_baseline"] = cpu_baseline_line(w)
             except Exception as ex:   # a reported baseline, not the product
                 line["cpu_baseline"] = {"value": None, "error": str(ex)}
         print(json.dumps(line))
+
+
+def roofline_traffic(kname, w):
+    """DRAM bytes per launch of the dominant kernel from the ncu captures
+    summarised under profiles/ (one small launch captured, scaled to this
+    workload's launch by the tiles it processes); None without a capture."""
+    return None
 
 
 def main():
@@ -502,6 +619,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--parallelism", default="shared", choices=["shared", "replicas"],
+                    help="N > 1: share one gradient (NCCL all-reduce) or run N replicas")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison step")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")

@@ -18,19 +18,20 @@ from . import capi
 ENERGY_KEYS = ("ss_aa", "ss_bb", "os", "total")
 
 
-def allreduce_gradient(g: capi.Gradient, group=None) -> capi.Gradient:
+def allreduce_gradient(g: capi.Gradient, group=None, device=None) -> capi.Gradient:
     """Sum of the ranks' partial gradients, on every rank.
 
     Works on the numpy results of ``Context.mp2_gradient`` (reduced as CPU
-    tensors, so the process group needs a CPU backend such as gloo) and on the
-    CUDA tensors of ``Context.mp2_gradient_torch`` (NCCL).  Timings in
+    tensors, so the process group needs a CPU backend such as gloo, or staged
+    through ``device`` -- a CUDA device for NCCL -- and returned as numpy) and
+    on the CUDA tensors of ``Context.mp2_gradient_torch`` (NCCL).  Timings in
     ``g.energy`` stay this rank's own."""
     import torch
     import torch.distributed as dist
 
     parts = [x for x in (g.dC_a, g.deps_a, g.dC_b, g.deps_b) if x is not None]
     on_torch = isinstance(g.dC_a, torch.Tensor)
-    dev = g.dC_a.device if on_torch else torch.device("cpu")
+    dev = g.dC_a.device if on_torch else torch.device(device if device is not None else "cpu")
     e = torch.tensor([float(g.energy[k]) for k in ENERGY_KEYS], dtype=torch.float64, device=dev)
     flat = torch.cat([e] + [(x if on_torch else torch.from_numpy(np.asarray(x))).reshape(-1).to(dev, torch.float64)
                             for x in parts])
@@ -44,7 +45,7 @@ def allreduce_gradient(g: capi.Gradient, group=None) -> capi.Gradient:
         piece = flat[off:off + n].reshape(tuple(x.shape))
         off += n
         if not on_torch:
-            piece = piece.numpy().copy(order="F" if np.asarray(x).flags.f_contiguous and x.ndim == 2 else "C")
+            piece = piece.cpu().numpy().copy(order="F" if np.asarray(x).flags.f_contiguous and x.ndim == 2 else "C")
         out.append(piece)
     it = iter(out)
     dC_a = next(it)
