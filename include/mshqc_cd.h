@@ -191,6 +191,20 @@ MSHQC_CD_API int mshqc_cd_mp2_energy(mshqc_cd_ctx* ctx, int kind, int precision,
  * 2 = ab (oa*ob).  Row-major [i][j]. */
 MSHQC_CD_API int mshqc_cd_pair_energies(mshqc_cd_ctx* ctx, int block, double* out, int where);
 
+/* Amplitudes of a block of pairs for the consumers of the reference's stored
+ * t2: CholeskyRMP2Result::t2 (reference include/mshqc/cholesky_rmp2.h:32-49,
+ * filled in src/mp2/cholesky_rmp2.cc:118-153, read by CholeskyRMP3) and
+ * CholeskyUMP2::compute_t2_amplitudes (src/mp2/cholesky_ump2.cc:471-556).
+ * FP64, the reference's convention in every block:
+ *   t_ij^ab = (ia|jb) / (e_i + e_j - e_a - e_b), 0 where |D| < 1e-12.
+ * block 0: alpha-alpha (the restricted amplitudes), 1: beta-beta,
+ * 2: alpha-beta.  Pairs i0 <= i < i0 + ni, j0 <= j < j0 + nj; out holds
+ * ni * nj * vx * vy doubles, element ((i - i0) nj + (j - j0)) vx vy + a vy + b
+ * (vx, vy: virtual counts of the two spins).  Runs the FP64 transforms
+ * first when needed. */
+MSHQC_CD_API int mshqc_cd_get_t2_block(mshqc_cd_ctx* ctx, int block, int64_t i0, int64_t ni, int64_t j0,
+                                       int64_t nj, double* out, int where);
+
 /* --- backward (exact differentiation; no reference counterpart) ------- */
 /* Energy and its exact derivatives with respect to the orbitals and the
  * orbital energies.  dC_a/dC_b: N*N column-major; deps_a/deps_b: N; any

@@ -19,7 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmshqc_cuda.so")
 
-CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_omp2.cu", "cd_vectors.cu", "cd_decompose.cu", "cd_noalloc.cu"]
+CUDA_SOURCES = ["cd_abi.cu", "cd_mp2.cu", "cd_omp2.cu", "cd_vectors.cu", "cd_decompose.cu", "cd_noalloc.cu",
+                "cd_t2.cu"]
 # host-only C++ (the AO integral engine), compiled by g++ with OpenMP
 HOST_SOURCES = ["ao_integrals.cc"]
 HOST_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-fopenmp", "-march=x86-64-v3"]

@@ -86,6 +86,7 @@ SIGNATURES = {
                                     _vp, _vp, _i32]),
     "mshqc_cd_omp2": (_i32, [_vp, ctypes.POINTER(Omp2Config), _vp, _vp, _i32, ctypes.POINTER(Omp2Result)]),
     "mshqc_cd_rmp2_energy_noalloc": (_i32, [_vp, _vp, _i64, _i64, _i64, _vp, _vp]),
+    "mshqc_cd_get_t2_block": (_i32, [_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i32]),
 }
 
 _lib = None
@@ -283,6 +284,21 @@ class Context:
         rows, cols = {0: (oa, oa), 1: (ob, ob), 2: (oa, ob)}[block]
         out = np.empty((rows, cols), dtype=np.float64)
         _check(self._lib.mshqc_cd_pair_energies(self._h, block, _ptr(out), HOST))
+        return out
+
+    def t2_block(self, block: int = 0, i0: int = 0, ni: int | None = None, j0: int = 0,
+                 nj: int | None = None) -> np.ndarray:
+        """FP64 amplitudes t[i, j, a, b] = (ia|jb)/D of pairs i0 <= i < i0+ni,
+        j0 <= j < j0+nj (block 0 alpha-alpha / restricted, 1 beta-beta,
+        2 alpha-beta), as an (ni, nj, vx, vy) array."""
+        oa, ob = self.nocc
+        ox = ob if block == 1 else oa
+        oy = oa if block == 0 else ob
+        ni = ox - i0 if ni is None else ni
+        nj = oy - j0 if nj is None else nj
+        vx, vy = self.nbf - ox, self.nbf - oy
+        out = np.empty((ni, nj, vx, vy), dtype=np.float64)
+        _check(self._lib.mshqc_cd_get_t2_block(self._h, block, i0, ni, j0, nj, _ptr(out), HOST))
         return out
 
     # -- backward ---------------------------------------------------------
