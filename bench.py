@@ -24,8 +24,11 @@ F_E = v^2 M o (o + 1) (integral tiles of the unique pairs i <= j),
 F_G = 2 v^2 M o^2 (Gamma), F_Tt = 2 M N o (N + 2 v) (transposed transforms);
 an energy-only step is F_T + F_E.  `e2e` = the same metric through the C ABI
 from host buffers, copies inside the timed region.  With --gpus N > 1 the
-ranks share one gradient (mshqc_cd_set_partition, NCCL all-reduce of the
-shares); --parallelism replicas runs N independent copies instead.
+ranks share one gradient (mshqc_cd_set_partition: block pairs of the
+backward; mshqc_cd_set_collectives: the half and transposed transforms over
+occupied orbitals with an NCCL all-gather of B and reduce-scatter of Gamma;
+an NCCL all-reduce of the shares); --parallelism replicas runs N
+independent copies instead.
 
 The reference arm (--impl reference) runs the reference's own CPU code
 (oracle/_ref, compiled from its sources) on a bounded sample of the workload:
@@ -405,6 +408,7 @@ def bench_gpu(args, w, rank, world, local_rank):
         ctx.set_vectors(L_dev)
     if shared:
         ctx.set_partition(rank, world)
+        ctx.set_collectives(*shard.nccl_collectives(dev))   # transforms shared over occupied orbitals
 
     def step(context, precision, C, eps):
         context.set_orbitals(capi.ALPHA, C, eps, o)            # new orbitals: full recompute
@@ -512,6 +516,7 @@ def bench_gpu(args, w, rank, world, local_rank):
         ctx_h.set_stream(stream.cuda_stream)
         if shared:
             ctx_h.set_partition(rank, world)
+            ctx_h.set_collectives(*shard.nccl_collectives(dev))
         L_np = None if gen else L_host.numpy()
 
         def step_e2e():

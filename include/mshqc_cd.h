@@ -119,6 +119,30 @@ MSHQC_CD_API int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream);
  * mshqc_cd_mp2_energy and the OMP2 entry points are not partitioned.
  * (0, 1) is the default: everything on this context. */
 MSHQC_CD_API int mshqc_cd_set_partition(mshqc_cd_ctx* ctx, int rank, int nranks);
+/* Collective operations for a shared gradient, supplied by the host (no
+ * counterpart in the reference).  Both run on the calling thread and act on
+ * device memory in the order of `stream` (the context's stream; the host may
+ * also synchronize it): `buf` holds nranks chunks of `count` doubles.
+ *   allgather       chunk `rank` of every rank's buf to all ranks (in place);
+ *   reduce_scatter  the sum over ranks of chunk r of buf lands in chunk r of
+ *                   rank r's buf (in place; other chunks may be overwritten).
+ * NCCL's in-place ncclAllGather / ncclReduceScatter on buf match these
+ * (recvbuff = buf, sendbuff = buf + rank * count).  Return 0, or nonzero to
+ * fail the call (MSHQC_CD_ERR_STATE). */
+typedef struct {
+    int (*allgather)(double* buf, int64_t count, void* stream, void* user);
+    int (*reduce_scatter)(double* buf, int64_t count, void* stream, void* user);
+    void* user;
+} mshqc_cd_collectives;
+/* With collectives set and a partition of nranks > 1, mshqc_cd_mp2_gradient
+ * also shares the half transforms and the transposed transforms: rank r
+ * transforms the occupied orbitals [r p, (r + 1) p) of each spin
+ * (p = ceil(nocc / nranks)) and allgather completes the MO vectors B on every
+ * rank; after the backward, reduce_scatter gives rank r the complete Gamma
+ * of its orbitals and its transposed transforms the columns of dE/dC they
+ * reach.  The returned shares still add up to the full result.  NULL
+ * clears them (the transforms then run in full on every rank). */
+MSHQC_CD_API int mshqc_cd_set_collectives(mshqc_cd_ctx* ctx, const mshqc_cd_collectives* ops);
 /* Bytes of device memory the context holds. */
 MSHQC_CD_API int mshqc_cd_device_bytes(mshqc_cd_ctx* ctx, int64_t* bytes);
 /* Number of kernels this context has launched so far. */

@@ -59,6 +59,15 @@ _vp = ctypes.c_void_p
 _i32 = ctypes.c_int
 _i64 = ctypes.c_int64
 # name -> (restype, argtypes); the set of exported entry points
+COLLECTIVE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int64, ctypes.c_void_p,
+                                 ctypes.c_void_p)
+
+
+class Collectives(ctypes.Structure):
+    """mshqc_cd_collectives (include/mshqc_cd.h)."""
+    _fields_ = [("allgather", COLLECTIVE_FN), ("reduce_scatter", COLLECTIVE_FN), ("user", ctypes.c_void_p)]
+
+
 SIGNATURES = {
     "mshqc_cd_ctx_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
     "mshqc_cd_ctx_destroy": (_i32, [_vp]),
@@ -87,6 +96,7 @@ SIGNATURES = {
     "mshqc_cd_omp2": (_i32, [_vp, ctypes.POINTER(Omp2Config), _vp, _vp, _i32, ctypes.POINTER(Omp2Result)]),
     "mshqc_cd_rmp2_energy_noalloc": (_i32, [_vp, _vp, _i64, _i64, _i64, _vp, _vp]),
     "mshqc_cd_get_t2_block": (_i32, [_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i32]),
+    "mshqc_cd_set_collectives": (_i32, [_vp, ctypes.POINTER(Collectives)]),
 }
 
 _lib = None
@@ -180,6 +190,35 @@ class Context:
         """Compute only share `rank` of `nranks` of the gradient's backward
         (sum the shares' energies and derivatives over the ranks)."""
         _check(self._lib.mshqc_cd_set_partition(self._h, int(rank), int(nranks)))
+        return self
+
+    def set_collectives(self, allgather, reduce_scatter):
+        """Host collectives for a shared gradient (mshqc_cd_set_collectives):
+        allgather(ptr, count, stream) and reduce_scatter(ptr, count, stream)
+        act in place on `nranks * count` doubles of device memory at the
+        integer address ptr, in the order of the CUDA stream handle `stream`.
+        With a partition of more than one rank the half transforms and the
+        transposed transforms are then shared too.  None clears them.  An
+        exception in a callback fails the library call and is re-raised."""
+        if allgather is None:
+            self._coll = None
+            _check(self._lib.mshqc_cd_set_collectives(self._h, None))
+            return self
+        self._coll_error = None
+
+        def wrap(fn):
+            def cb(buf, count, stream, user):
+                try:
+                    fn(ctypes.cast(buf, ctypes.c_void_p).value, int(count), stream or 0)
+                    return 0
+                except BaseException as ex:   # reported through the library's status
+                    self._coll_error = ex
+                    return 1
+            return COLLECTIVE_FN(cb)
+
+        cbs = (wrap(allgather), wrap(reduce_scatter))
+        self._coll = (cbs, Collectives(cbs[0], cbs[1], None))
+        _check(self._lib.mshqc_cd_set_collectives(self._h, ctypes.byref(self._coll[1])))
         return self
 
     def device_bytes(self) -> int:
@@ -302,6 +341,15 @@ class Context:
         return out
 
     # -- backward ---------------------------------------------------------
+    def _grad_call(self, fn):
+        self._coll_error = None
+        rc = fn()
+        err = getattr(self, "_coll_error", None)
+        if err is not None:
+            self._coll_error = None
+            raise err
+        _check(rc)
+
     def mp2_gradient(self, kind: int = RESTRICTED, precision: int = FP64) -> Gradient:
         N = self.nbf
         e = Energy()
@@ -312,7 +360,7 @@ class Context:
             deb = np.zeros(N, dtype=np.float64)
         else:
             dCb = deb = None
-        _check(self._lib.mshqc_cd_mp2_gradient(
+        self._grad_call(lambda: self._lib.mshqc_cd_mp2_gradient(
             self._h, kind, precision, ctypes.byref(e), _ptr(dCa),
             _ptr(dCb) if dCb is not None else None, _ptr(dea),
             _ptr(deb) if deb is not None else None, HOST))
@@ -331,7 +379,7 @@ class Context:
         dCt = [torch.empty((N, N), dtype=torch.float64, device=device) for _ in range(nspin)]
         de = [torch.empty(N, dtype=torch.float64, device=device) for _ in range(nspin)]
         torch.cuda.current_stream(device).synchronize()
-        _check(self._lib.mshqc_cd_mp2_gradient(
+        self._grad_call(lambda: self._lib.mshqc_cd_mp2_gradient(
             self._h, kind, precision, ctypes.byref(e), _ptr(dCt[0]), _ptr(dCt[1]) if nspin == 2 else None,
             _ptr(de[0]), _ptr(de[1]) if nspin == 2 else None, DEVICE))
         # the library writes column-major dC: the tensor holds dC^T

@@ -310,6 +310,15 @@ int mshqc_cd_set_partition(mshqc_cd_ctx* ctx, int rank, int nranks) {
     return MSHQC_CD_OK;
 }
 
+int mshqc_cd_set_collectives(mshqc_cd_ctx* ctx, const mshqc_cd_collectives* ops) {
+    CD_CHECK_CTX();
+    if (ops && (!ops->allgather || !ops->reduce_scatter))
+        return set_error(MSHQC_CD_ERR_ARG, "collectives need allgather and reduce_scatter");
+    ctx->coll_set = ops != nullptr;
+    ctx->coll = ops ? *ops : mshqc_cd_collectives{};
+    return MSHQC_CD_OK;
+}
+
 int mshqc_cd_stage_times(mshqc_cd_ctx* ctx, double* ms_out, int n_out) {
     CD_CHECK_CTX();
     if (!ms_out || n_out < 0) return set_error(MSHQC_CD_ERR_ARG, "bad output");

@@ -117,6 +117,11 @@ struct mshqc_cd_ctx {
     bool part_active = false;
     int64_t part_next = 0;
     std::vector<uint8_t> part_owned;
+    // host collectives (mshqc_cd_set_collectives): with them the transforms
+    // of a partitioned gradient are shared over occupied orbitals too
+    mshqc_cd_collectives coll{};
+    bool coll_set = false;
+    int64_t Y_lo = 0, Y_hi = 0;     // occupied orbitals whose half-transformed vectors Y holds
 
     std::vector<double> pair_energy[3];  // host copies, row-major [i][j]
 

@@ -108,14 +108,50 @@ int require_inputs(mshqc_cd_ctx* ctx, int spin) {
     return MSHQC_CD_OK;
 }
 
-// FP64 half transform of one spin into the padded [i][a][Q] layout.
-int transform_f64(mshqc_cd_ctx* ctx, int spin) {
+// ---------------------------------------------------------------------------
+// transforms shared over occupied orbitals (partition + host collectives)
+// ---------------------------------------------------------------------------
+// Rank r of R owns the occupied orbitals [r p, min(o, (r + 1) p)),
+// p = ceil(o / R); per-orbital buffers (B, Gamma) then hold R p rows so that
+// every rank's chunk has the same size for the collectives.
+bool sharded(const mshqc_cd_ctx* ctx) { return ctx->part_active && ctx->coll_set && ctx->part_size > 1; }
+int64_t shard_p(const mshqc_cd_ctx* ctx, int64_t o) { return cdiv(o, ctx->part_size); }
+void shard_range(const mshqc_cd_ctx* ctx, int64_t o, int64_t* lo, int64_t* hi) {
+    if (!sharded(ctx)) {
+        *lo = 0;
+        *hi = o;
+        return;
+    }
+    const int64_t p = shard_p(ctx, o);
+    *lo = std::min(o, (int64_t)ctx->part_rank * p);
+    *hi = std::min(o, *lo + p);
+}
+int64_t b_rows(const mshqc_cd_ctx* ctx, int64_t o) { return sharded(ctx) ? shard_p(ctx, o) * ctx->part_size : o; }
+
+int run_collective(mshqc_cd_ctx* ctx, bool gather, double* buf, int64_t count) {
+    int (*fn)(double*, int64_t, void*, void*) = gather ? ctx->coll.allgather : ctx->coll.reduce_scatter;
+    const int rc = fn(buf, count, (void*)ctx->stream, ctx->coll.user);
+    if (rc != 0)
+        return set_error(MSHQC_CD_ERR_STATE, std::string(gather ? "allgather" : "reduce_scatter") +
+                                                 " callback failed with " + std::to_string(rc));
+    return MSHQC_CD_OK;
+}
+
+// FP64 half transform of one spin into the padded [i][a][Q] layout, for the
+// occupied orbitals [lo, hi) (Y holds rows i - lo; B rows outside stay zero).
+int transform_f64(mshqc_cd_ctx* ctx, int spin, int64_t lo, int64_t hi) {
     SpinState& s = ctx->spin[spin];
-    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o;
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, ni = hi - lo;
     const int64_t vp = round_up(v, 64);
-    CD_ALLOC(ctx->Y, sizeof(double) * (size_t)o * M * N, false);
-    CD_ALLOC(s.B64, sizeof(double) * (size_t)o * vp * Mp, true);
+    CD_ALLOC(ctx->Y, sizeof(double) * (size_t)std::max<int64_t>(1, ni) * M * N, false);
+    CD_ALLOC(s.B64, sizeof(double) * (size_t)b_rows(ctx, o) * vp * Mp, true);
     s.vp = vp;
+    ctx->Y_spin = spin;
+    ctx->Y_lo = lo;
+    ctx->Y_hi = hi;
+    s.B64_valid = true;
+    s.B64_prec = MSHQC_CD_FP64;
+    if (ni <= 0) return MSHQC_CD_OK;
     const double* C = s.C.as<double>();
     // Y[i][(Q,nu)] = sum_mu C[mu,i] L[Q][nu*N + mu], one chunk of Q at a time
     const int64_t qc = vectors_chunk_size(ctx);
@@ -124,11 +160,11 @@ int transform_f64(mshqc_cd_ctx* ctx, int spin) {
         const double* Lc = nullptr;
         CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
         GemmF64Args g1{};
-        g1.M = (int)o;
+        g1.M = (int)ni;
         g1.N = (int)(mc * N);
         g1.K = (int)N;
         g1.batch = 1;
-        g1.A = C;  g1.lda = N;  g1.sA = 0;
+        g1.A = C + lo * N;  g1.lda = N;  g1.sA = 0;
         g1.B = Lc;  g1.ldb = N;  g1.sB = 0;
         g1.C = ctx->Y.as<double>() + Q0 * N;  g1.ldc = M * N;  g1.sC = 0;
         g1.alpha = 1.0;  g1.beta = 0.0;
@@ -140,16 +176,13 @@ int transform_f64(mshqc_cd_ctx* ctx, int spin) {
     g2.M = (int)v;
     g2.N = (int)M;
     g2.K = (int)N;
-    g2.batch = (int)o;
+    g2.batch = (int)ni;
     g2.A = C + o * N;  g2.lda = N;  g2.sA = 0;
     g2.B = ctx->Y.as<double>();  g2.ldb = N;  g2.sB = M * N;
-    g2.C = s.B64.as<double>();  g2.ldc = Mp;  g2.sC = vp * Mp;
+    g2.C = s.B64.as<double>() + lo * vp * Mp;  g2.ldc = Mp;  g2.sC = vp * Mp;
     g2.alpha = 1.0;  g2.beta = 0.0;
     CD_CUDA(gemm_f64(g2, true, true, ctx->stream));
     ctx->launches++;
-    s.B64_valid = true;
-    s.B64_prec = MSHQC_CD_FP64;
-    ctx->Y_spin = spin;
     return MSHQC_CD_OK;
 }
 
@@ -168,25 +201,31 @@ bool int8_transform_enabled(const mshqc_cd_ctx* ctx) {
 // B_i = C_vir^T Y_i^T in batches of occupied orbitals.  Accuracy of the
 // slices (about 2^-33 of the row maxima per term), not FP64 rounding: used by
 // the mixed-precision path only.
-int transform_i8(mshqc_cd_ctx* ctx, int spin) {
+int transform_i8(mshqc_cd_ctx* ctx, int spin, int64_t lo, int64_t hi) {
     using namespace ozaki;
     SpinState& s = ctx->spin[spin];
-    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o;
+    const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, ni = hi - lo;
     const int64_t vp = round_up(v, 64);
-    CD_ALLOC(ctx->Y, sizeof(double) * (size_t)o * M * N, false);
-    CD_ALLOC(s.B64, sizeof(double) * (size_t)o * vp * Mp, true);
+    CD_ALLOC(ctx->Y, sizeof(double) * (size_t)std::max<int64_t>(1, ni) * M * N, false);
+    CD_ALLOC(s.B64, sizeof(double) * (size_t)b_rows(ctx, o) * vp * Mp, true);
     CD_ALLOC(ctx->oz_flag, sizeof(int) * 2, true);
     s.vp = vp;
+    ctx->Y_spin = spin;
+    ctx->Y_lo = lo;
+    ctx->Y_hi = hi;
+    s.B64_valid = true;
+    s.B64_prec = MSHQC_CD_FP16X3;
+    if (ni <= 0) return MSHQC_CD_OK;
     int* err = ctx->oz_flag.as<int>();
     const double* C = s.C.as<double>();
-    // rows of C^T: occupied orbitals (first product), virtual orbitals (second)
-    OzakiOperand Ao = ozaki_operand(o, N, BM, 1), Av = ozaki_operand(v, N, BM, 1);
+    // rows of C^T: occupied orbitals of the slice (first product), virtual orbitals (second)
+    OzakiOperand Ao = ozaki_operand(ni, N, BM, 1), Av = ozaki_operand(v, N, BM, 1);
     const size_t ao_bytes = operand_bytes(Ao.Rp, Ao.Kp);
     CD_ALLOC(ctx->oz_a, ao_bytes + operand_bytes(Av.Rp, Av.Kp), false);
     CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(Ao.Rp + Av.Rp), false);
     Ao.q = ctx->oz_a.as<int8_t>();  Ao.e = ctx->oz_ea.as<int>();
     Av.q = Ao.q + ao_bytes;         Av.e = Ao.e + Ao.Rp;
-    CD_CUDA(ozaki_slice(C, N, 0, Ao, ctx->num_sms, ctx->stream));
+    CD_CUDA(ozaki_slice(C + lo * N, N, 0, Ao, ctx->num_sms, ctx->stream));
     CD_CUDA(ozaki_slice(C + o * N, N, 0, Av, ctx->num_sms, ctx->stream));
     ctx->launches += 2;
     // Y[i][(Q,nu)] = sum_mu C[mu,i] L[Q][nu*N + mu]
@@ -211,14 +250,14 @@ int transform_i8(mshqc_cd_ctx* ctx, int spin) {
     }
     // B[i][a][Q] = sum_nu C[nu, o+a] Y[i][Q][nu], a batch of orbitals i at a time
     const int64_t per_i = (int64_t)operand_bytes(padded_rows(M, BN), padded_k(N));
-    const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)kSliceBytes / per_i));
-    for (int64_t i0 = 0; i0 < o; i0 += ib) {
-        const int64_t nb = std::min(ib, o - i0);
+    const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(ni, (int64_t)kSliceBytes / per_i));
+    for (int64_t i0 = lo; i0 < hi; i0 += ib) {
+        const int64_t nb = std::min(ib, hi - i0);
         OzakiOperand By = ozaki_operand(M, N, BN, (int)nb);
         CD_ALLOC(ctx->oz_b, operand_bytes(By.Rp, By.Kp) * (size_t)nb, false);
         CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(By.Rp * nb), false);
         By.q = ctx->oz_b.as<int8_t>();  By.e = ctx->oz_eb.as<int>();
-        CD_CUDA(ozaki_slice(ctx->Y.as<double>() + i0 * M * N, N, M * N, By, ctx->num_sms, ctx->stream));
+        CD_CUDA(ozaki_slice(ctx->Y.as<double>() + (i0 - lo) * M * N, N, M * N, By, ctx->num_sms, ctx->stream));
         CD_CUDA(ozaki_gemm(Av, true, By, false, s.B64.as<double>() + i0 * vp * Mp, Mp, vp * Mp, 1.0, 0.0, err,
                            ctx->num_sms, ctx->stream));
         ctx->launches += 2;
@@ -229,9 +268,6 @@ int transform_i8(mshqc_cd_ctx* ctx, int spin) {
     if (herr)
         return set_error(MSHQC_CD_ERR_TIMEOUT, "int8 tensor-core transform gave up waiting (site " +
                                                    std::to_string(herr) + ")");
-    s.B64_valid = true;
-    s.B64_prec = MSHQC_CD_FP16X3;
-    ctx->Y_spin = spin;
     return MSHQC_CD_OK;
 }
 
@@ -569,10 +605,15 @@ int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
     // an FP64 request never reuses int8-slice products; a mixed one reuses either
     if (!s.B64_valid || (precision == MSHQC_CD_FP64 && s.B64_prec != MSHQC_CD_FP64)) {
         begin_stage(ctx, ST_TRANSFORM);
+        // shared over ranks: this rank's orbitals, then the gather of all
+        int64_t lo = 0, hi = s.nocc;
+        shard_range(ctx, s.nocc, &lo, &hi);
         if (precision == MSHQC_CD_FP16X3 && int8_transform_enabled(ctx))
-            CD_RC(transform_i8(ctx, spin));
+            CD_RC(transform_i8(ctx, spin, lo, hi));
         else
-            CD_RC(transform_f64(ctx, spin));
+            CD_RC(transform_f64(ctx, spin, lo, hi));
+        if (sharded(ctx))
+            CD_RC(run_collective(ctx, true, s.B64.as<double>(), shard_p(ctx, s.nocc) * s.vp * ctx->Mp));
         end_stage(ctx);
         s.B16_valid = false;
     }
@@ -638,32 +679,56 @@ namespace {
 // dE/dB = scale * Gamma (4 restricted, 2 unrestricted):
 // dC[nu, o+a] = sum_{i,Q} dE/dB[i][a][Q] Y[i][Q][nu],
 // dC[mu, i]   = sum_{Q,nu} L[Q][nu][mu] sum_a dE/dB[i][a][Q] C[nu, o+a].
+// The transforms shared over ranks: rank r's Gamma rows [lo, hi) are
+// completed by the reduce-scatter, and its transposed transforms cover those
+// orbitals only (dC's other occupied columns zero); unshared: [0, o).
+// Makes sure the buffer Y holds the half-transformed vectors of [lo, hi).
+int transposed_prepare(mshqc_cd_ctx* ctx, int spin, bool i8, int64_t* lo, int64_t* hi, double* dC) {
+    SpinState& s = ctx->spin[spin];
+    shard_range(ctx, s.nocc, lo, hi);
+    if (sharded(ctx))
+        CD_RC(run_collective(ctx, false, ctx->gam[spin].as<double>(), shard_p(ctx, s.nocc) * s.vp * ctx->Mp));
+    if (ctx->Y_spin != spin || ctx->Y_lo != *lo || ctx->Y_hi != *hi) {
+        // recomputing Y rewrites B as well; shared, only this rank's rows of it
+        if (i8)
+            CD_RC(transform_i8(ctx, spin, *lo, *hi));
+        else
+            CD_RC(transform_f64(ctx, spin, *lo, *hi));
+        if (sharded(ctx)) s.B64_valid = false;
+    }
+    if (*hi - *lo < s.nocc) CD_CUDA(cudaMemsetAsync(dC, 0, sizeof(double) * (size_t)(s.nocc * ctx->N), ctx->stream));
+    if (*hi <= *lo)
+        CD_CUDA(cudaMemsetAsync(dC + s.nocc * ctx->N, 0, sizeof(double) * (size_t)((ctx->N - s.nocc) * ctx->N),
+                                ctx->stream));
+    return MSHQC_CD_OK;
+}
+
 int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC) {
     SpinState& s = ctx->spin[spin];
     const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
     // Y[i][Q][nu] (half-transformed vectors of this spin) is needed
-    if (ctx->Y_spin != spin) {
-        s.B64_valid = false;
-        CD_RC(transform_f64(ctx, spin));
-    }
+    int64_t lo = 0, hi = o;
+    CD_RC(transposed_prepare(ctx, spin, false, &lo, &hi, dC));
+    const int64_t ni = hi - lo;
+    if (ni <= 0) return MSHQC_CD_OK;
     const double* C = s.C.as<double>();
     const double* Gm = ctx->gam[spin].as<double>();
     // dC[nu, o+a] = scale sum_{i,Q} Gamma[i][a][Q] Y[i][Q][nu]   (row-major [a][nu] == column-major dC)
-    for (int64_t i = 0; i < o; ++i) {
+    for (int64_t i = lo; i < hi; ++i) {
         GemmF64Args g{};
         g.M = (int)v;  g.N = (int)N;  g.K = (int)M;  g.batch = 1;
         g.A = Gm + i * vp * Mp;  g.lda = Mp;  g.sA = 0;
-        g.B = ctx->Y.as<double>() + i * M * N;  g.ldb = N;  g.sB = 0;
+        g.B = ctx->Y.as<double>() + (i - lo) * M * N;  g.ldb = N;  g.sB = 0;
         g.C = dC + o * N;  g.ldc = N;  g.sC = 0;
-        g.alpha = scale;  g.beta = i == 0 ? 0.0 : 1.0;
+        g.alpha = scale;  g.beta = i == lo ? 0.0 : 1.0;
         CD_CUDA(gemm_f64(g, true, false, ctx->stream));
         ctx->launches++;
     }
     // W[i][Q][nu] = sum_a Gamma[i][a][Q] C[nu, o+a]   (into the Y buffer)
     {
         GemmF64Args g{};
-        g.M = (int)M;  g.N = (int)N;  g.K = (int)v;  g.batch = (int)o;
-        g.A = Gm;  g.lda = Mp;  g.sA = vp * Mp;
+        g.M = (int)M;  g.N = (int)N;  g.K = (int)v;  g.batch = (int)ni;
+        g.A = Gm + lo * vp * Mp;  g.lda = Mp;  g.sA = vp * Mp;
         g.B = C + o * N;  g.ldb = N;  g.sB = 0;
         g.C = ctx->Y.as<double>();  g.ldc = N;  g.sC = M * N;
         g.alpha = 1.0;  g.beta = 0.0;
@@ -680,10 +745,10 @@ int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC)
             const double* Lc = nullptr;
             CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
             GemmF64Args g{};
-            g.M = (int)o;  g.N = (int)N;  g.K = (int)(mc * N);  g.batch = 1;
+            g.M = (int)ni;  g.N = (int)N;  g.K = (int)(mc * N);  g.batch = 1;
             g.A = ctx->Y.as<double>() + Q0 * N;  g.lda = M * N;  g.sA = 0;
             g.B = Lc;  g.ldb = N;  g.sB = 0;
-            g.C = dC;  g.ldc = N;  g.sC = 0;
+            g.C = dC + lo * N;  g.ldc = N;  g.sC = 0;
             g.alpha = scale;  g.beta = Q0 == 0 ? 0.0 : 1.0;
             CD_CUDA(gemm_f64(g, true, false, ctx->stream));
             ctx->launches++;
@@ -695,15 +760,15 @@ int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC)
     // reduction adds up
     {
         const int64_t K = M * N;
-        const int64_t tiles = cdiv(o, 64) * cdiv(N, 64);
+        const int64_t tiles = cdiv(ni, 64) * cdiv(N, 64);
         const int64_t S = std::max<int64_t>(1, std::min<int64_t>(256, cdiv(4 * ctx->num_sms, tiles)));
         const int64_t Kc = (K / S) / 16 * 16, Krem = K - S * Kc;   // even chunks keep 16-byte copies
-        CD_ALLOC(ctx->W, sizeof(double) * (size_t)(S * o * N), false);
+        CD_ALLOC(ctx->W, sizeof(double) * (size_t)(S * ni * N), false);
         GemmF64Args g{};
-        g.M = (int)o;  g.N = (int)N;  g.K = (int)Kc;  g.batch = (int)S;
+        g.M = (int)ni;  g.N = (int)N;  g.K = (int)Kc;  g.batch = (int)S;
         g.A = ctx->Y.as<double>();  g.lda = M * N;  g.sA = Kc;
         g.B = ctx->L.as<double>();  g.ldb = N;  g.sB = Kc * N;
-        g.C = ctx->W.as<double>();  g.ldc = N;  g.sC = o * N;
+        g.C = ctx->W.as<double>();  g.ldc = N;  g.sC = ni * N;
         g.alpha = 1.0;  g.beta = 0.0;
         CD_CUDA(gemm_f64(g, true, false, ctx->stream));
         ctx->launches++;
@@ -716,8 +781,8 @@ int transposed_transforms(mshqc_cd_ctx* ctx, int spin, double scale, double* dC)
             CD_CUDA(gemm_f64(t, true, false, ctx->stream));
             ctx->launches++;
         }
-        sum_partials_kernel<<<(unsigned)cdiv(o * N, 256), 256, 0, ctx->stream>>>(
-            ctx->W.as<double>(), (int)S, o * N, scale, dC);
+        sum_partials_kernel<<<(unsigned)cdiv(ni * N, 256), 256, 0, ctx->stream>>>(
+            ctx->W.as<double>(), (int)S, ni * N, scale, dC + lo * N);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
@@ -753,10 +818,10 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
     using namespace ozaki;
     SpinState& s = ctx->spin[spin];
     const int64_t N = ctx->N, M = ctx->M, Mp = ctx->Mp, o = s.nocc, v = N - o;
-    if (ctx->Y_spin != spin) {
-        s.B64_valid = false;
-        CD_RC(transform_i8(ctx, spin));
-    }
+    int64_t lo = 0, hi = o;
+    CD_RC(transposed_prepare(ctx, spin, true, &lo, &hi, dC));
+    const int64_t ni = hi - lo;
+    if (ni <= 0) return MSHQC_CD_OK;
     const int64_t vp = s.vp;
     const double* C = s.C.as<double>();
     const double* Gm = ctx->gam[spin].as<double>();
@@ -768,23 +833,23 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
         const size_t pa = operand_bytes(padded_rows(v, BM), padded_k(M));
         const size_t pb = operand_bytes(padded_rows(N, BN), padded_k(M));
         const size_t pp = sizeof(double) * (size_t)(v * N);
-        const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(2 * kSliceBytes / (pa + pb + pp))));
+        const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(ni, (int64_t)(2 * kSliceBytes / (pa + pb + pp))));
         CD_ALLOC(ctx->oz_a, pa * ib, false);
         CD_ALLOC(ctx->oz_b, pb * ib, false);
         CD_ALLOC(ctx->oz_p, pp * ib, false);
         CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(v, BM) * ib), false);
         CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(padded_rows(N, BN) * ib), false);
-        for (int64_t i0 = 0; i0 < o; i0 += ib) {
-            const int64_t nb = std::min(ib, o - i0);
+        for (int64_t i0 = lo; i0 < hi; i0 += ib) {
+            const int64_t nb = std::min(ib, hi - i0);
             OzakiOperand A = ozaki_operand(v, M, BM, (int)nb), B = ozaki_operand(N, M, BN, (int)nb);
             A.q = ctx->oz_a.as<int8_t>();  A.e = ctx->oz_ea.as<int>();
             B.q = ctx->oz_b.as<int8_t>();  B.e = ctx->oz_eb.as<int>();
             CD_CUDA(ozaki_slice(Gm + i0 * vp * Mp, Mp, vp * Mp, A, ctx->num_sms, ctx->stream));
-            CD_CUDA(ozaki_slice_t(Y + i0 * M * N, N, M * N, B, ctx->stream));
+            CD_CUDA(ozaki_slice_t(Y + (i0 - lo) * M * N, N, M * N, B, ctx->stream));
             CD_CUDA(ozaki_gemm(A, false, B, false, ctx->oz_p.as<double>(), N, v * N, 1.0, 0.0, err, ctx->num_sms,
                                ctx->stream));
             ctx->launches += 5;
-            CD_RC(sum_batches(ctx, ctx->oz_p.as<double>(), (int)nb, v * N, scale, i0 > 0, dC + o * N));
+            CD_RC(sum_batches(ctx, ctx->oz_p.as<double>(), (int)nb, v * N, scale, i0 > lo, dC + o * N));
         }
     }
     // W[i][Q][nu] into the Y buffer: A = Gamma_i^T (rows Q, K = a, strided by Mp),
@@ -792,7 +857,7 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
     {
         OzakiOperand B = ozaki_operand(N, v, BN, 1);
         const size_t pa = operand_bytes(padded_rows(M, BM), padded_k(v));
-        const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(o, (int64_t)(kSliceBytes / pa)));
+        const int64_t ib = std::max<int64_t>(1, std::min<int64_t>(ni, (int64_t)(kSliceBytes / pa)));
         CD_ALLOC(ctx->oz_a, pa * ib, false);
         CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(M, BM) * ib), false);
         CD_ALLOC(ctx->oz_b, operand_bytes(B.Rp, B.Kp), false);
@@ -800,12 +865,12 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
         B.q = ctx->oz_b.as<int8_t>();  B.e = ctx->oz_eb.as<int>();
         CD_CUDA(ozaki_slice_t(C + o * N, N, 0, B, ctx->stream));
         ctx->launches += 3;
-        for (int64_t i0 = 0; i0 < o; i0 += ib) {
-            const int64_t nb = std::min(ib, o - i0);
+        for (int64_t i0 = lo; i0 < hi; i0 += ib) {
+            const int64_t nb = std::min(ib, hi - i0);
             OzakiOperand A = ozaki_operand(M, v, BM, (int)nb);
             A.q = ctx->oz_a.as<int8_t>();  A.e = ctx->oz_ea.as<int>();
             CD_CUDA(ozaki_slice_t(Gm + i0 * vp * Mp, Mp, vp * Mp, A, ctx->stream));
-            CD_CUDA(ozaki_gemm(A, false, B, true, Y + i0 * M * N, N, M * N, 1.0, 0.0, err, ctx->num_sms,
+            CD_CUDA(ozaki_gemm(A, false, B, true, Y + (i0 - lo) * M * N, N, M * N, 1.0, 0.0, err, ctx->num_sms,
                                ctx->stream));
             ctx->launches += 4;
         }
@@ -813,9 +878,9 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
     }
     // dC[mu, i]: A = W_Q (rows i, K = nu), B = L_Q (rows mu, K = nu, strided by N)
     {
-        const size_t pa = operand_bytes(padded_rows(o, BM), padded_k(N));
+        const size_t pa = operand_bytes(padded_rows(ni, BM), padded_k(N));
         const size_t pb = operand_bytes(padded_rows(N, BN), padded_k(N));
-        const size_t pp = sizeof(double) * (size_t)(o * N);
+        const size_t pp = sizeof(double) * (size_t)(ni * N);
         const int64_t nq_max = std::max<int64_t>(1, (int64_t)(2 * kSliceBytes / (pa + pb + pp)));
         const int64_t qc = vectors_chunk_size(ctx);
         // (batches are the z dimension of the transposed-slicing grid)
@@ -823,7 +888,7 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
         CD_ALLOC(ctx->oz_a, pa * nq, false);
         CD_ALLOC(ctx->oz_b, pb * nq, false);
         CD_ALLOC(ctx->oz_p, pp * nq, false);
-        CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(o, BM) * nq), false);
+        CD_ALLOC(ctx->oz_ea, sizeof(int) * (size_t)(padded_rows(ni, BM) * nq), false);
         CD_ALLOC(ctx->oz_eb, sizeof(int) * (size_t)(padded_rows(N, BN) * nq), false);
         for (int64_t Q0 = 0; Q0 < M; Q0 += qc) {
             const int64_t mc = std::min(qc, M - Q0);
@@ -831,15 +896,15 @@ int transposed_transforms_i8(mshqc_cd_ctx* ctx, int spin, double scale, double* 
             CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
             for (int64_t q0 = 0; q0 < mc; q0 += nq) {
                 const int64_t nb = std::min(nq, mc - q0);
-                OzakiOperand A = ozaki_operand(o, N, BM, (int)nb), B = ozaki_operand(N, N, BN, (int)nb);
+                OzakiOperand A = ozaki_operand(ni, N, BM, (int)nb), B = ozaki_operand(N, N, BN, (int)nb);
                 A.q = ctx->oz_a.as<int8_t>();  A.e = ctx->oz_ea.as<int>();
                 B.q = ctx->oz_b.as<int8_t>();  B.e = ctx->oz_eb.as<int>();
                 CD_CUDA(ozaki_slice(Y + (Q0 + q0) * N, M * N, N, A, ctx->num_sms, ctx->stream));
                 CD_CUDA(ozaki_slice_t(Lc + q0 * N * N, N, N * N, B, ctx->stream));
-                CD_CUDA(ozaki_gemm(A, false, B, false, ctx->oz_p.as<double>(), N, o * N, 1.0, 0.0, err,
+                CD_CUDA(ozaki_gemm(A, false, B, false, ctx->oz_p.as<double>(), N, ni * N, 1.0, 0.0, err,
                                    ctx->num_sms, ctx->stream));
                 ctx->launches += 5;
-                CD_RC(sum_batches(ctx, ctx->oz_p.as<double>(), (int)nb, o * N, scale, Q0 + q0 > 0, dC));
+                CD_RC(sum_batches(ctx, ctx->oz_p.as<double>(), (int)nb, ni * N, scale, Q0 + q0 > 0, dC + lo * N));
             }
         }
     }
@@ -875,7 +940,7 @@ int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double*
                                        kPartF64Budget);
     CD_ALLOC(ctx->amp, per_i * bi, false);
     // zeroed: with a partition the blocks of other ranks stay zero
-    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)o * vp * Mp, ctx->part_active);
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)b_rows(ctx, o) * vp * Mp, ctx->part_active);
     CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
     const int64_t units_per_i = (int64_t)o * nb * nb;
     CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), ctx->part_active);
@@ -1225,7 +1290,7 @@ int gradient_restricted_tc(mshqc_cd_ctx* ctx, double* dC, double* deps, double* 
     const int64_t N = ctx->N, Mp = ctx->Mp, RQ = round_up(ctx->M, 256);
     const uint16_t* bt[2] = {nullptr, nullptr};
     CD_RC(make_bt(ctx, 0, ctx->BT, RQ, &bt[0], &bt[1]));
-    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)d.o * s.vp * Mp, true);
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)b_rows(ctx, d.o) * s.vp * Mp, true);
     CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
     CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
@@ -1264,8 +1329,8 @@ int gradient_unrestricted(mshqc_cd_ctx* ctx, int precision, double* const dC[2],
         CD_RC(make_bt(ctx, 0, ctx->BT, RQ, &bta[0], &bta[1]));
         CD_RC(make_bt(ctx, 1, ctx->BT_b, RQ, &btb[0], &btb[1]));
     }
-    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)da.o * da.vp * Mp, true);
-    CD_ALLOC(ctx->gam[1], sizeof(double) * (size_t)db.o * db.vp * Mp, true);
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)b_rows(ctx, da.o) * da.vp * Mp, true);
+    CD_ALLOC(ctx->gam[1], sizeof(double) * (size_t)b_rows(ctx, db.o) * db.vp * Mp, true);
     for (int s = 0; s < 2; ++s) CD_CUDA(cudaMemsetAsync(deps[s], 0, sizeof(double) * N, ctx->stream));
     CD_ALLOC(ctx->flag, sizeof(int) * 4, true);
     CD_ALLOC(ctx->totals, sizeof(double) * 8, false);

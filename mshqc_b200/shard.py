@@ -5,9 +5,13 @@ share with ``Context.set_partition(rank, world)`` and calls the gradient; the
 library computes that rank's block pairs of occupied orbitals (the
 independent (i, j) tiles of the backward, the bulk of the work) and returns
 their energy, dE/dC and dE/deps.  ``allreduce_gradient`` then adds the
-shares over the ranks: the one exchange step of the path, 3 + 2 N^2 + 2 N
-doubles at most, by ``torch.distributed.all_reduce`` (NCCL for CUDA tensors,
-gloo for host ones).
+shares over the ranks, 3 + 2 N^2 + 2 N doubles at most, by
+``torch.distributed.all_reduce`` (NCCL for CUDA tensors, gloo for host ones).
+With ``Context.set_collectives(*nccl_collectives(device))`` the half
+transforms and the transposed transforms are shared over occupied orbitals
+as well: an all-gather of the MO vectors B after the forward transforms and
+a reduce-scatter of Gamma before the transposed ones, in place on the
+library's device buffers.
 """
 from __future__ import annotations
 
@@ -16,6 +20,67 @@ import numpy as np
 from . import capi
 
 ENERGY_KEYS = ("ss_aa", "ss_bb", "os", "total")
+
+
+class _DeviceArray:
+    """count doubles of device memory at address ptr, for torch.as_tensor
+    (zero copy, through the CUDA array interface)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None, "stream": None}
+
+
+def _device_tensor(ptr, count, device):
+    import torch
+    return torch.as_tensor(_DeviceArray(ptr, count), device=device)
+
+
+def nccl_collectives(device, group=None):
+    """(allgather, reduce_scatter) for Context.set_collectives over an NCCL
+    process group: in place on the library's buffer, on the library's
+    stream (torch.distributed all_gather_into_tensor / reduce_scatter_tensor
+    with the rank's chunk as input / output)."""
+    import torch
+    import torch.distributed as dist
+
+    def run(ptr, count, stream, gather):
+        world = dist.get_world_size(group)
+        rank = dist.get_rank(group)
+        full = _device_tensor(ptr, world * count, device)
+        mine = full[rank * count:(rank + 1) * count]
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=device)):
+            if gather:
+                dist.all_gather_into_tensor(full, mine, group=group)
+            else:
+                dist.reduce_scatter_tensor(mine, full, op=dist.ReduceOp.SUM, group=group)
+
+    return (lambda p, c, st: run(p, c, st, True)), (lambda p, c, st: run(p, c, st, False))
+
+
+def staged_collectives(device, group=None):
+    """The same operations staged through host memory over a CPU process
+    group (gloo): for ranks that share one GPU in tests, or jobs without
+    NCCL.  The library's stream is synchronized before the copies."""
+    import torch
+    import torch.distributed as dist
+
+    def run(ptr, count, stream, gather):
+        torch.cuda.ExternalStream(stream, device=device).synchronize()
+        world = dist.get_world_size(group)
+        rank = dist.get_rank(group)
+        full = _device_tensor(ptr, world * count, device)
+        host = full.cpu()
+        if gather:
+            parts = [torch.empty(count, dtype=torch.float64) for _ in range(world)]
+            dist.all_gather(parts, host[rank * count:(rank + 1) * count].clone(), group=group)
+            full.copy_(torch.cat(parts))
+        else:
+            dist.all_reduce(host, op=dist.ReduceOp.SUM, group=group)
+            full[rank * count:(rank + 1) * count].copy_(host[rank * count:(rank + 1) * count])
+        torch.cuda.synchronize(device)
+
+    return (lambda p, c, st: run(p, c, st, True)), (lambda p, c, st: run(p, c, st, False))
 
 
 def allreduce_gradient(g: capi.Gradient, group=None, device=None) -> capi.Gradient:
