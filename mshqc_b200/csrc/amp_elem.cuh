@@ -64,7 +64,30 @@ struct AmpElemArgs {
     // cpocc [lp][c], and amp_chunks_combine_kernel adds the chunks in order
     int nchunk;
     double* cpcol; double* cpart; double* cpocc;
+    // tri: a diagonal block pair of the symmetric modes with only its pairs
+    // ii <= jj (nbi == nbj, local pairs in the order of vtile_pair): an
+    // off-diagonal pair stands for (i, j) and (j, i) -- weight 2 -- and its
+    // transposed amplitudes go into the same operand (Thi / Tlo = Ahi / Alo)
+    int tri;
 };
+
+namespace amp_detail {
+// local pair lp -> (ii, jj), row-major or the upper triangle (see tri)
+__device__ __forceinline__ void local_pair(const AmpElemArgs& p, int lp, int& ii, int& jj) {
+    if (!p.tri) {
+        ii = lp / p.nbj;
+        jj = lp % p.nbj;
+        return;
+    }
+    int r = lp, i = 0;
+    while (r >= p.nbi - i) {
+        r -= p.nbi - i;
+        ++i;
+    }
+    ii = i;
+    jj = i + r;
+}
+}  // namespace amp_detail
 
 namespace amp_detail {
 // blocked K-major element offset of (row R, column k) in the operand layout
@@ -105,7 +128,10 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
     const int ta = p.rsx / 32, tb = p.ksy / 32;
     const int R = p.nchunk > 1 ? p.nchunk : 1;
     const int lp = (int)(blockIdx.x / R), ch = (int)(blockIdx.x % R);
-    const int ii = lp / p.nbj, jj = lp % p.nbj;
+    int ii, jj;
+    amp_detail::local_pair(p, lp, ii, jj);
+    const double wgt = p.tri ? (ii < jj ? 2.0 : 1.0) : p.wgt;
+    const bool write_t = p.Thi != nullptr && !(p.tri && ii == jj);
     const int xb0 = ch * ta / R, xb1 = (ch + 1) * ta / R;   // this CTA's row tiles
     const int i = p.i0 + ii, j = p.j0 + jj;
     const long long pair = (long long)i * p.oy + j;          // over all occupied rows
@@ -194,7 +220,7 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
                     const long long kc = (long long)jj * p.ksy + b0 + g * 8;
                     const long long off = amp_detail::blocked_offset(R, kc, p.nkA);
                     amp_detail::store_hilo8(&T[r][g * 8], p.Ahi + off, p.Alo + off);
-                } else if (p.Thi) {
+                } else if (write_t) {
                     const int w = threadIdx.x - 128;
                     const int r = w >> 2, g = w & 3;   // r: b offset, g: group of 8 a
                     const long long R = (long long)jj * p.ksy + b0 + r;
@@ -210,7 +236,7 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
                 double c = 0.0;
 #pragma unroll
                 for (int w = 0; w < 8; ++w) c += colpart[w][tx];
-                pcol[b0 + tx] = (xb == xb0 ? 0.0 : pcol[b0 + tx]) + p.wgt * c;
+                pcol[b0 + tx] = (xb == xb0 ? 0.0 : pcol[b0 + tx]) + wgt * c;
             }
             __syncthreads();   // Vt, Wt, T, colpart are refilled by the next tile
         }
@@ -220,7 +246,7 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
                 double rs = rsum[k];
 #pragma unroll
                 for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
-                if (tx == 0) prow[a0 + ty * 4 + k] = p.wgt * rs;
+                if (tx == 0) prow[a0 + ty * 4 + k] = wgt * rs;
             }
         }
     }
@@ -241,11 +267,11 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
             r += red_r[w];
         }
         if (R == 1) {
-            p.partial[pair] = p.wgt * e;
-            if (p.pocc) p.pocc[pair] = p.wgt * r;
+            p.partial[pair] = wgt * e;
+            if (p.pocc) p.pocc[pair] = wgt * r;
         } else {
-            p.cpart[(long long)lp * R + ch] = p.wgt * e;
-            if (p.pocc) p.cpocc[(long long)lp * R + ch] = p.wgt * r;
+            p.cpart[(long long)lp * R + ch] = wgt * e;
+            if (p.pocc) p.cpocc[(long long)lp * R + ch] = wgt * r;
         }
     }
 }
@@ -258,7 +284,9 @@ static __global__ void amp_chunks_combine_kernel(AmpElemArgs p, int npl) {
     if (idx >= (long long)npl * p.ksy) return;
     const int lp = (int)(idx / p.ksy), b = (int)(idx % p.ksy);
     const int R = p.nchunk;
-    const long long pair = (long long)(p.i0 + lp / p.nbj) * p.oy + p.j0 + lp % p.nbj;
+    int ii, jj;
+    amp_detail::local_pair(p, lp, ii, jj);
+    const long long pair = (long long)(p.i0 + ii) * p.oy + p.j0 + jj;
     if (p.pcol) {
         double sc = 0.0;
         for (int c = 0; c < R; ++c) sc += p.cpcol[((long long)lp * R + c) * p.ksy + b];

@@ -1125,6 +1125,10 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             if (!owns_next(ctx)) continue;
             const int nJ = (int)std::min<int64_t>(bJ, dy.o - J0);
             const bool mirror = !kSym || J0 != I0;
+            // a diagonal block pair computes its pairs i <= j only; the
+            // element-wise pass writes the (j, i) amplitudes as transposes
+            const bool tri = kSym && J0 == I0;
+            const int npl = tri ? nI * (nI + 1) / 2 : nI * nJ;
             VtileArgs a{};
             a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
             a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
@@ -1138,7 +1142,8 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             a.nbx = (int)(dx.VR / 128);  a.nby = (int)dy.nby;  a.VS = (int)dy.VS;
             a.S = ctx->W.as<float>();
             a.err = ctx->flag.as<int>();
-            const int64_t vunits = (int64_t)nI * nJ * a.nbx * a.nby;
+            a.tri = tri ? 1 : 0;
+            const int64_t vunits = (int64_t)npl * a.nbx * a.nby;
             const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
             begin_stage(ctx, ST_AMPLITUDE);
             vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
@@ -1159,12 +1164,15 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             if (mirror) {
                 e.Thi = ctx->ampT.as<uint16_t>();  e.Tlo = ctx->ampT2.as<uint16_t>();
                 e.nkT = (long long)nI * dx.VR / 16;
+            } else if (tri) {
+                e.Thi = e.Ahi;  e.Tlo = e.Alo;  e.nkT = e.nkA;
+                e.tri = 1;
             }
             e.partial = partial;
             e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
             // split each pair's row tiles over several CTAs when the block
             // pair alone does not fill the GPU several times over
-            const int ta = (int)(dx.VR / 32), npl = (int)(nI * nJ);
+            const int ta = (int)(dx.VR / 32);
             int nch = 1;
             while (nch < 4 && 2 * nch <= ta && (int64_t)npl * nch < 8LL * ctx->num_sms) nch *= 2;
             e.nchunk = nch;
@@ -1385,8 +1393,11 @@ int plan_partition(mshqc_cd_ctx* ctx, int kind, int precision) {
             const int64_t nI = std::min(bI, dx.o - I0);
             for (int64_t J0 = sym ? I0 : 0; J0 < dy.o; J0 += bJ) {
                 const int64_t nJ = std::min(bJ, dy.o - J0);
-                const bool mirror = !sym || J0 != I0;
-                cost.push_back((double)nI * nJ * (mirror ? 3.0 : 2.0));
+                // integral tiles of the pairs computed + Gamma products
+                if (sym && J0 == I0)
+                    cost.push_back(0.5 * (double)nI * (nI + 1) + (double)nI * nI);
+                else
+                    cost.push_back(3.0 * nI * nJ);
             }
         }
     };

@@ -42,7 +42,25 @@ struct VtileArgs {
     int VS;                 // staging columns per orbital j (nby * 256)
     float* S;               // staging [nbi * VR][nbj * VS]
     int* err;
+    int tri;                // 1: only the pairs ii <= jj of a diagonal block (nbi == nbj)
 };
+
+// Local pair pr -> (ii, jj): row-major over nbi x nbj, or over the upper
+// triangle ii <= jj (rows of nbi - ii pairs) when p.tri.
+__device__ __forceinline__ void vtile_pair(const VtileArgs& p, long long pr, int& ii, int& jj) {
+    if (!p.tri) {
+        ii = (int)(pr / p.nbj);
+        jj = (int)(pr % p.nbj);
+        return;
+    }
+    int r = (int)pr, i = 0;
+    while (r >= p.nbi - i) {
+        r -= p.nbi - i;
+        ++i;
+    }
+    ii = i;
+    jj = i + r;
+}
 
 namespace vtile_tc {
 constexpr int BM = 128, BN = 256, KC = 16, KS = 2, STAGES = 4, THREADS = 192;
@@ -93,7 +111,8 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
 
     // unit u -> (ii, j, x, y): pair-major so that concurrent CTAs share slabs
     const long long per_pair = (long long)p.nbx * p.nby;
-    const long long units = (long long)p.nbi * p.nbj * per_pair;
+    const long long npl = p.tri ? (long long)p.nbi * (p.nbi + 1) / 2 : (long long)p.nbi * p.nbj;
+    const long long units = npl * per_pair;
     const long long first = blockIdx.x, step = gridDim.x;
     const int nk = p.nqc;
 
@@ -102,7 +121,9 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
             uint32_t stage = 0, phase = 0, fill_phase = 0, filled = 0;
             for (long long u = first; u < units && !*abort_flag; u += step) {
                 const long long pr = u / per_pair, bb = u % per_pair;
-                const int i = p.i0 + (int)(pr / p.nbj), j = p.j0 + (int)(pr % p.nbj);
+                int ii, jj;
+                vtile_pair(p, pr, ii, jj);
+                const int i = p.i0 + ii, j = p.j0 + jj;
                 const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
                 // slab bases at Q step 0 (256-row blocks of nqc steps, 4096 elements a step)
                 const size_t nq = (size_t)p.nqc;
@@ -195,7 +216,9 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
         uint32_t acc_phase = 0;
         for (long long u = first; u < units; u += step) {
             const long long pr = u / per_pair, bb = u % per_pair;
-            const int ii = (int)(pr / p.nbj), jj = (int)(pr % p.nbj), i = p.i0 + ii, j = p.j0 + jj;
+            int ii, jj;
+            vtile_pair(p, pr, ii, jj);
+            const int i = p.i0 + ii, j = p.j0 + jj;
             const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
             const int a = x * BM + row, b0 = y * BN;
             for (int c = etid; c < BN; c += 128) {
