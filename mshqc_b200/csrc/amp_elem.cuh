@@ -148,8 +148,9 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int r = ty + 8 * k;
-            v[k] = Srow[(long long)(a0 + r) * p.ldS + b0 + tx];
-            if (kW) w[k] = Srow[(long long)(b0 + r) * p.ldS + a0 + tx];
+            // streaming loads: the staging is read here and never again
+            v[k] = __ldcs(Srow + (long long)(a0 + r) * p.ldS + b0 + tx);
+            if (kW) w[k] = __ldcs(Srow + (long long)(b0 + r) * p.ldS + a0 + tx);
         }
     };
     TS vn[4], wn[4];

@@ -259,10 +259,13 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
                     out[k] = arow ? (float)V : 0.0f;
                 }
                 if (a < p.VR) {
+                    // streaming stores (evict first): the staging is read once
+                    // by the element-wise pass, and must not push the
+                    // operands that other CTAs still read out of L2
                     float4* d4 = reinterpret_cast<float4*>(dst + c0);
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
-                        d4[k] = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
+                        __stcs(d4 + k, make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]));
                 }
             }
             tc_fence_before();
