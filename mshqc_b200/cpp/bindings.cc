@@ -40,6 +40,14 @@ Matrix to_matrix(const farray& a) {
     return m;
 }
 
+// (i,j,a,b) column-major amplitudes as an (o1, o2, v1, v2) Fortran-ordered array
+py::object t2_to_numpy(const std::vector<double>& t, int o1, int o2, int v1, int v2) {
+    if (t.empty()) return py::none();
+    py::array_t<double, py::array::f_style> a({(py::ssize_t)o1, (py::ssize_t)o2, (py::ssize_t)v1, (py::ssize_t)v2});
+    std::memcpy(a.mutable_data(), t.data(), t.size() * sizeof(double));
+    return std::move(a);
+}
+
 py::array_t<double> vec_to_numpy(const Vector& v) {
     py::array_t<double> a((py::ssize_t)v.size());
     if (!v.empty()) std::memcpy(a.mutable_data(), v.data(), sizeof(double) * v.size());
@@ -164,7 +172,15 @@ PYBIND11_MODULE(_mshqc, m) {
         .def_readonly("e_total", &foundation::CholeskyRMP2Result::e_total)
         .def_readonly("n_chol_vectors", &foundation::CholeskyRMP2Result::n_chol_vectors)
         .def_readonly("n_occ", &foundation::CholeskyRMP2Result::n_occ)
-        .def_readonly("n_virt", &foundation::CholeskyRMP2Result::n_virt);
+        .def_readonly("n_virt", &foundation::CholeskyRMP2Result::n_virt)
+        .def_property_readonly("t2", [](const foundation::CholeskyRMP2Result& r) {
+            return t2_to_numpy(r.t2, r.n_occ, r.n_occ, r.n_virt, r.n_virt);
+        })
+        .def_property_readonly("chol_vectors", [](const foundation::CholeskyRMP2Result& r) {
+            py::list out;
+            for (const auto& v : r.chol_vectors) out.append(vec_to_numpy(v));
+            return out;
+        });
 
     py::class_<CholeskyRMP2>(m, "CholeskyRMP2")
         .def(py::init([](const py::object&, const py::object& basis, const py::object& integrals,
@@ -211,6 +227,28 @@ PYBIND11_MODULE(_mshqc, m) {
         }))
         .def("compute", &CholeskyUMP2::compute, "Compute UMP2 energy using Cholesky vectors")
         .def("compute_t2_amplitudes", &CholeskyUMP2::compute_t2_amplitudes)
+        .def_property_readonly("L_ia_alpha", [](const CholeskyUMP2& u) {
+            py::list out;
+            for (const auto& m : u.L_ia_alpha()) out.append(to_numpy(m));
+            return out;
+        })
+        .def_property_readonly("L_ia_beta", [](const CholeskyUMP2& u) {
+            py::list out;
+            for (const auto& m : u.L_ia_beta()) out.append(to_numpy(m));
+            return out;
+        })
+        .def_property_readonly("t2_aa", [](const CholeskyUMP2& u) {
+            const int a = u.n_occ_alpha(), va = u.n_basis() - a;
+            return t2_to_numpy(u.t2_aa(), a, a, va, va);
+        })
+        .def_property_readonly("t2_bb", [](const CholeskyUMP2& u) {
+            const int b = u.n_occ_beta(), vb = u.n_basis() - b;
+            return t2_to_numpy(u.t2_bb(), b, b, vb, vb);
+        })
+        .def_property_readonly("t2_ab", [](const CholeskyUMP2& u) {
+            const int a = u.n_occ_alpha(), b = u.n_occ_beta();
+            return t2_to_numpy(u.t2_ab(), a, b, u.n_basis() - a, u.n_basis() - b);
+        })
         .def("get_cholesky", &CholeskyUMP2::get_cholesky, py::return_value_policy::reference_internal);
 
     // ---- CD-OMP2

@@ -3,6 +3,7 @@
 #include "mshqc_b200.hpp"
 
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <iostream>
@@ -35,6 +36,36 @@ void set_vectors(const DeviceContext& ctx, const CholeskyERI& chol) {
     if (chol.n_vectors() == 0) throw std::runtime_error("no Cholesky vectors");
     check(mshqc_cd_set_vectors(ctx.get(), chol.vectors().data(), chol.n_basis(), chol.n_vectors(),
                                MSHQC_CD_LAYOUT_FULL, MSHQC_CD_HOST));
+}
+
+size_t t2_max_bytes() {
+    const char* env = std::getenv("MSHQC_T2_MAX_BYTES");
+    return env ? (size_t)std::strtoull(env, nullptr, 10) : (size_t(8) << 30);
+}
+
+// amplitudes of one spin block, (i,j,a,b) column-major; empty above the limit
+std::vector<double> fetch_t2(const DeviceContext& ctx, int block, int ox, int oy, int vx, int vy) {
+    if (8.0 * ox * oy * (double)vx * vy > (double)t2_max_bytes()) return {};
+    std::vector<double> t2((size_t)ox * oy * vx * vy), row((size_t)oy * vx * vy);
+    for (int i = 0; i < ox; ++i) {
+        check(mshqc_cd_get_t2_block(ctx.get(), block, i, 1, 0, oy, row.data(), MSHQC_CD_HOST));
+        for (int j = 0; j < oy; ++j)
+            for (int a = 0; a < vx; ++a)
+                for (int b = 0; b < vy; ++b)
+                    t2[(size_t)i + (size_t)ox * (j + (size_t)oy * (a + (size_t)vx * b))] =
+                        row[((size_t)j * vx + a) * vy + b];
+    }
+    return t2;
+}
+
+std::vector<Matrix> fetch_mo_vectors(const DeviceContext& ctx, int spin, int nocc, int nvir, int nvec) {
+    std::vector<double> B((size_t)nocc * nvir * nvec);
+    check(mshqc_cd_transform(ctx.get(), spin, MSHQC_CD_FP64, B.data(), MSHQC_CD_HOST));
+    std::vector<Matrix> out(nvec, Matrix(nocc, nvir));
+    for (int i = 0; i < nocc; ++i)
+        for (int a = 0; a < nvir; ++a)
+            for (int q = 0; q < nvec; ++q) out[q](i, a) = B[((size_t)i * nvir + a) * nvec + q];
+    return out;
 }
 
 }  // namespace
@@ -142,6 +173,8 @@ foundation::CholeskyRMP2Result CholeskyRMP2::compute() {
     r.e_rhf = rhf_.energy_total;
     r.e_corr = e.total;
     r.e_total = r.e_rhf + r.e_corr;
+    r.t2 = fetch_t2(ctx, 0, nocc_, nocc_, nvirt_, nvirt_);
+    r.chol_vectors = chol_->get_L_vectors();
     r.n_chol_vectors = chol_->n_vectors();
     r.n_occ = nocc_;
     r.n_virt = nvirt_;
@@ -194,6 +227,9 @@ CholeskyUMP2Result CholeskyUMP2::compute() {
     r.memory_mb = chol->storage_bytes() / 1024.0 / 1024.0;
     r.time_transform_s = e.ms_transform / 1e3;
     r.time_energy_s = e.ms_energy / 1e3;
+    const int nva = nbf_ - uhf_.n_occ_alpha, nvb = nbf_ - uhf_.n_occ_beta;
+    L_ia_alpha_ = fetch_mo_vectors(ctx, MSHQC_CD_ALPHA, uhf_.n_occ_alpha, nva, chol->n_vectors());
+    L_ia_beta_ = fetch_mo_vectors(ctx, MSHQC_CD_BETA, uhf_.n_occ_beta, nvb, chol->n_vectors());
     if (config_.print_level > 0)
         std::cout << "[CholeskyUMP2] E(corr) = " << e.total << " Eh (ss_aa " << e.ss_aa << ", ss_bb " << e.ss_bb
                   << ", os " << e.os << ")\n";
@@ -201,8 +237,18 @@ CholeskyUMP2Result CholeskyUMP2::compute() {
 }
 
 void CholeskyUMP2::compute_t2_amplitudes() {
-    throw std::runtime_error(
-        "CholeskyUMP2::compute_t2_amplitudes: the GPU path never stores the o^2 v^2 amplitudes");
+    const int na = uhf_.n_occ_alpha, nb = uhf_.n_occ_beta, va = nbf_ - na, vb = nbf_ - nb;
+    require_orbitals(uhf_.C_alpha, uhf_.orbital_energies_alpha, nbf_, na, "CholeskyUMP2 (alpha)");
+    require_orbitals(uhf_.C_beta, uhf_.orbital_energies_beta, nbf_, nb, "CholeskyUMP2 (beta)");
+    DeviceContext ctx(config_.device);
+    set_vectors(ctx, chol_);
+    check(mshqc_cd_set_orbitals(ctx.get(), MSHQC_CD_ALPHA, uhf_.C_alpha.data(), uhf_.orbital_energies_alpha.data(),
+                                na, MSHQC_CD_HOST));
+    check(mshqc_cd_set_orbitals(ctx.get(), MSHQC_CD_BETA, uhf_.C_beta.data(), uhf_.orbital_energies_beta.data(),
+                                nb, MSHQC_CD_HOST));
+    t2_aa_ = fetch_t2(ctx, 0, na, na, va, va);
+    t2_bb_ = fetch_t2(ctx, 1, nb, nb, vb, vb);
+    t2_ab_ = fetch_t2(ctx, 2, na, nb, va, vb);
 }
 
 // ---------------------------------------------------------------------------

@@ -16,8 +16,11 @@
 //    does not count them, cholesky_eri.h:76-83);
 //  * CholeskyRMP2Config / CholeskyUMP2Config carry `precision` (0 = FP64,
 //    1 = mixed FP16x3) and all configs carry `device`;
-//  * CholeskyRMP2Result carries no t2 (o^2 v^2 doubles) and no copy of the
-//    vectors; CholeskyUMP2::compute_t2_amplitudes throws for the same reason;
+//  * the stored amplitudes (CholeskyRMP2Result::t2, CholeskyUMP2's t2 after
+//    compute_t2_amplitudes, both (i,j,a,b) column-major as Eigen stores
+//    them) come from mshqc_cd_get_t2_block in FP64 and stay empty above
+//    MSHQC_T2_MAX_BYTES (default 8 GiB), where the reference would run out
+//    of host memory;
 //  * an empty set of reused vectors makes CholeskyOMP2 throw
 //    std::runtime_error where the reference calls exit(1) (cholesky_omp2.cc:62-65).
 #pragma once
@@ -123,6 +126,8 @@ private:
 namespace foundation {
 struct CholeskyRMP2Result {
     double e_rhf = 0.0, e_corr = 0.0, e_total = 0.0;
+    std::vector<double> t2;              // o*o*v*v, element (i,j,a,b) at i + o (j + o (a + v b))
+    std::vector<Vector> chol_vectors;    // the AO vectors, for reuse by MP3
     int n_chol_vectors = 0, n_occ = 0, n_virt = 0;
 };
 }  // namespace foundation
@@ -175,8 +180,18 @@ public:
     CholeskyUMP2(const SCFResult& uhf_result, int n_basis, std::shared_ptr<IntegralSource> integrals,
                  const CholeskyUMP2Config& config, const CholeskyERI& cholesky);
     CholeskyUMP2Result compute();
-    void compute_t2_amplitudes();   // throws: amplitudes are never stored
+    // t2_aa, t2_bb, t2_ab = (ia|jb)/D (reference cholesky_ump2.cc:471-556)
+    void compute_t2_amplitudes();
     const CholeskyERI& get_cholesky() const { return chol_; }
+    int n_occ_alpha() const { return uhf_.n_occ_alpha; }
+    int n_occ_beta() const { return uhf_.n_occ_beta; }
+    int n_basis() const { return nbf_; }
+    const std::vector<double>& t2_aa() const { return t2_aa_; }   // (i,j,a,b) column-major
+    const std::vector<double>& t2_bb() const { return t2_bb_; }
+    const std::vector<double>& t2_ab() const { return t2_ab_; }
+    // L^K_ia after compute(): [K](i, a) (the reference's L_ia_alpha_ / L_ia_beta_)
+    const std::vector<Matrix>& L_ia_alpha() const { return L_ia_alpha_; }
+    const std::vector<Matrix>& L_ia_beta() const { return L_ia_beta_; }
 
 private:
     SCFResult uhf_;
@@ -184,6 +199,8 @@ private:
     std::shared_ptr<IntegralSource> integrals_;
     CholeskyUMP2Config config_;
     CholeskyERI chol_;
+    std::vector<double> t2_aa_, t2_bb_, t2_ab_;
+    std::vector<Matrix> L_ia_alpha_, L_ia_beta_;
 };
 
 struct CholeskyOMP2Config {

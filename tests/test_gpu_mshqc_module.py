@@ -2,7 +2,9 @@
 reference's scripts use its classes: CholeskyERI -> CholeskyRMP2 /
 CholeskyUMP2 / CholeskyOMP2 -> compute(), against the reference's own
 results (golden fixtures made by running it).  Energies 1e-12 relative
-(1e-11 for the OMP2 loop), orbitals 1e-9."""
+(1e-11 for the OMP2 loop), orbitals 1e-9; the stored t2 of
+CholeskyRMP2Result and CholeskyUMP2's t2 / L_ia (what the reference's MP3
+classes read) 1e-12 of their largest element."""
 import numpy as np
 import pytest
 
@@ -52,6 +54,12 @@ def test_cholesky_rmp2_vs_reference(golden, name):
     assert abs(res.e_corr - g["e_corr"]) <= 1e-12 * abs(g["e_corr"])
     assert res.e_total == res.e_rhf + res.e_corr and res.e_rhf == -1.5
     assert (res.n_occ, res.n_virt, res.n_chol_vectors) == (o, N - o, g["L"].shape[0])
+    # the stored amplitudes and vectors the reference's CholeskyRMP3 reads
+    if "t2" in g.files:
+        assert res.t2.shape == g["t2"].shape
+        assert np.max(np.abs(res.t2 - g["t2"])) <= 1e-12 * np.max(np.abs(g["t2"]))
+    assert len(res.chol_vectors) == g["L"].shape[0]
+    assert np.array_equal(res.chol_vectors[0], g["L"][0])
 
 
 @pytest.mark.parametrize("name", ["ump2_n26_o6_5_m70", "ump2_n20_o4_3_m50"])
@@ -66,6 +74,22 @@ def test_cholesky_ump2_vs_reference(golden, name):
                       ("e_corr_total", "e_corr")):
         assert abs(getattr(res, attr) - g[key]) <= 1e-12 * abs(g[key]) + 1e-14, attr
     assert res.n_cholesky_vectors == g["L"].shape[0]
+    # the MO vectors and amplitudes the reference's CholeskyUMP3 reads
+    u = mshqc.CholeskyUMP2(scf(g["Ca"], g["ea"], na, g["Cb"], g["eb"], nb), N, None,
+                           quiet(mshqc.CholeskyUMP2Config()), chol)
+    u.compute()
+    u.compute_t2_amplitudes()
+    Ba = orc.transform(g["L"], g["Ca"], na)
+    Bb = orc.transform(g["L"], g["Cb"], nb)
+    assert len(u.L_ia_alpha) == g["L"].shape[0] and len(u.L_ia_beta) == g["L"].shape[0]
+    assert np.max(np.abs(np.stack(u.L_ia_alpha, axis=-1) - Ba)) <= 1e-12 * np.max(np.abs(Ba))
+    ea, eb = g["ea"], g["eb"]
+    for t, X, Y, ex, ey, ox, oy in ((u.t2_aa, Ba, Ba, ea, ea, na, na), (u.t2_bb, Bb, Bb, eb, eb, nb, nb),
+                                    (u.t2_ab, Ba, Bb, ea, eb, na, nb)):
+        gg = np.einsum("iaQ,jbQ->ijab", X, Y)
+        D = (ex[:ox, None, None, None] + ey[None, :oy, None, None] - ex[None, None, ox:, None]
+             - ey[None, None, None, oy:])
+        assert np.max(np.abs(t - gg / D)) <= 1e-12 * np.max(np.abs(gg / D))
 
 
 def test_cholesky_omp2_vs_reference(golden):
