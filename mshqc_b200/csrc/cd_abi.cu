@@ -83,6 +83,10 @@ cudaError_t DevBuf::reserve(size_t nbytes, bool zero, cudaStream_t st) {
     release();
     cudaError_t e = cudaMalloc(&p, nbytes);
     if (e != cudaSuccess) {
+        // the caller reports the failure; clear the runtime's last error so
+        // that the next cudaGetLastError() after a kernel launch does not
+        // return it again
+        (void)cudaGetLastError();
         p = nullptr;
         bytes = 0;
         return e;
