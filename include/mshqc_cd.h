@@ -29,6 +29,8 @@
 
 #include <stdint.h>
 
+#include "mshqc_ao.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -175,6 +177,19 @@ MSHQC_CD_API int mshqc_cd_set_vectors(mshqc_cd_ctx* ctx, const double* L, int64_
 MSHQC_CD_API int mshqc_cd_cholesky_decompose(mshqc_cd_ctx* ctx, const double* eri, int64_t nbf,
                                              double threshold, double* L_out, int64_t max_vectors,
                                              int64_t* n_vectors, int* converged, int where);
+/* Integral-direct pivoted Cholesky: DirectCholesky::compute (reference
+ * src/integrals/cholesky_direct.cc:32-187), without the N^4 ERI tensor.  The
+ * ERI diagonal and one ERI column per vector come from the host AO engine
+ * (include/mshqc_ao.h; `basis` as there), the pivot search (first index of
+ * the largest diagonal), the column reduction and the diagonal update
+ * (negatives above -1e-10 set to zero) run on the device.  Stops below the
+ * threshold, at a negative largest diagonal (*converged = 0 when it is
+ * below -1e-10) or after N^2 / 2 vectors.  The vectors become the context's
+ * (as after mshqc_cd_set_vectors) and, when L_out is not NULL, are copied
+ * there (max_vectors * N^2 doubles of room). */
+MSHQC_CD_API int mshqc_cd_cholesky_direct(mshqc_cd_ctx* ctx, const mshqc_ao_basis* basis,
+                                          double threshold, double* L_out, int64_t max_vectors,
+                                          int64_t* n_vectors, int* converged, int where);
 /* Synthetic Cholesky vectors generated on the device instead of uploaded
  * (no counterpart in the reference, which takes them as data): L^Q = sigma
  * 10^(-6 Q / nvec) (X^Q + X^Q^T)/2, X^Q standard normal: for mu <= nu one

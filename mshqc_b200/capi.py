@@ -97,6 +97,8 @@ SIGNATURES = {
     "mshqc_cd_rmp2_energy_noalloc": (_i32, [_vp, _vp, _i64, _i64, _i64, _vp, _vp]),
     "mshqc_cd_get_t2_block": (_i32, [_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i32]),
     "mshqc_cd_set_collectives": (_i32, [_vp, ctypes.POINTER(Collectives)]),
+    "mshqc_cd_cholesky_direct": (_i32, [_vp, _vp, ctypes.c_double, _vp, _i64, ctypes.POINTER(_i64),
+                                        ctypes.POINTER(_i32), _i32]),
 }
 
 _lib = None
@@ -276,6 +278,23 @@ class Context:
         conv = ctypes.c_int(0)
         _check(self._lib.mshqc_cd_cholesky_decompose(self._h, _ptr(E), N, float(threshold), _ptr(out), N * N,
                                                       ctypes.byref(m), ctypes.byref(conv), HOST))
+        self.nbf, self.nvec = N, int(m.value)
+        self.decompose_converged = bool(conv.value)
+        return out[:m.value].copy()
+
+    def cholesky_direct(self, basis, threshold: float = 1e-6):
+        """Integral-direct pivoted Cholesky over an ``ao.BasisSet``: the ERI
+        diagonal and columns from the host AO engine, the decomposition on
+        the device.  Returns the vectors (M, N*N); they become the
+        context's vectors."""
+        st, keep = basis._struct()
+        N = basis.n_basis_functions()
+        cap = N * N // 2 + 1
+        out = np.empty((cap, N * N), dtype=np.float64)
+        m = ctypes.c_int64(0)
+        conv = ctypes.c_int(0)
+        _check(self._lib.mshqc_cd_cholesky_direct(self._h, ctypes.addressof(st), float(threshold), _ptr(out), cap,
+                                                  ctypes.byref(m), ctypes.byref(conv), HOST))
         self.nbf, self.nvec = N, int(m.value)
         self.decompose_converged = bool(conv.value)
         return out[:m.value].copy()

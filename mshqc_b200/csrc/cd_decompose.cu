@@ -14,9 +14,11 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "cd_common.cuh"
 #include "cd_internal.h"
+#include "../../include/mshqc_ao.h"
 
 namespace mshqc_cd {
 namespace {
@@ -67,6 +69,28 @@ __global__ void chol_column_kernel(const double* __restrict__ eri, int64_t n2, c
     for (int k = 0; k < m; ++k) val = __dsub_rn(val, __dmul_rn(L[(int64_t)k * n2 + e], L[(int64_t)k * n2 + p]));
     const double nf = sqrt(Dp);
     out[e] = nf > 1e-12 ? val / nf : val;
+}
+
+// integral-direct variant: the column (e|p) arrives in out, is reduced in
+// place in the order of src/integrals/cholesky_direct.cc:180-186 and divided
+// by sqrt(D_p)
+__global__ void chol_direct_column_kernel(const double* __restrict__ L, int m, int64_t n2, int64_t p, double Dp,
+                                          double* __restrict__ out) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n2) return;
+    double val = out[e];
+    for (int k = 0; k < m; ++k) val = __dsub_rn(val, __dmul_rn(L[(int64_t)k * n2 + e], L[(int64_t)k * n2 + p]));
+    out[e] = val / sqrt(Dp);
+}
+
+// D -= L^2 with the direct variant's clamp: only small negatives (> -1e-10)
+// become zero (src/integrals/cholesky_direct.cc:130-134)
+__global__ void chol_direct_diag_update_kernel(double* __restrict__ D, const double* __restrict__ Lm, int64_t n2) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n2) return;
+    double d = __dsub_rn(D[e], __dmul_rn(Lm[e], Lm[e]));
+    if (d < 0.0 && d > -1e-10) d = 0.0;
+    D[e] = d;
 }
 
 __global__ void chol_diag_update_kernel(double* __restrict__ D, const double* __restrict__ Lm, int64_t n2) {
@@ -131,6 +155,77 @@ extern "C" MSHQC_CD_API int mshqc_cd_cholesky_decompose(mshqc_cd_ctx* ctx, const
     }
     *n_vectors = m;
     if (converged) *converged = m < n2 ? 1 : 0;
+    if (L_out) {
+        if (m > max_vectors)
+            return set_error(MSHQC_CD_ERR_ARG, "L_out holds " + std::to_string(max_vectors) + " vectors, " +
+                                                   std::to_string(m) + " were produced");
+        CD_RC(download(ctx, L_out, L, sizeof(double) * (size_t)(m * n2), where));
+    }
+    ctx->N = nbf;
+    ctx->M = m;
+    ctx->Mp = round_up(std::max<int64_t>(m, 1), 16);
+    ctx->L_set = m > 0;
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MSHQC_CD_OK;
+}
+
+// Integral-direct pivoted Cholesky (reference src/integrals/cholesky_direct.cc:
+// 32-187, DirectCholesky::compute): the ERI diagonal and, per vector, the one
+// ERI column of the pivot come from the host AO engine (mshqc_ao_*), the
+// pivot search, the column reduction and the diagonal update run on the
+// device.  Stops when the largest diagonal is below the threshold or
+// negative, or after N^2 / 2 vectors, as the reference does.
+extern "C" MSHQC_CD_API int mshqc_cd_cholesky_direct(mshqc_cd_ctx* ctx, const mshqc_ao_basis* basis,
+                                                     double threshold, double* L_out, int64_t max_vectors,
+                                                     int64_t* n_vectors, int* converged, int where) {
+    if (!ctx) return set_error(MSHQC_CD_ERR_ARG, "null context");
+    if (!basis || !n_vectors) return set_error(MSHQC_CD_ERR_ARG, "basis and n_vectors must be non-null");
+    if (!(threshold > 0.0)) return set_error(MSHQC_CD_ERR_ARG, "threshold must be positive");
+    if (where != MSHQC_CD_HOST && where != MSHQC_CD_DEVICE)
+        return set_error(MSHQC_CD_ERR_ARG, "unknown pointer location");
+    int64_t nbf = 0;
+    if (mshqc_ao_nbf(basis, &nbf) != MSHQC_AO_OK)
+        return set_error(MSHQC_CD_ERR_ARG, std::string("basis: ") + mshqc_ao_last_error());
+    DeviceGuard g(ctx->device);
+    const int64_t n2 = nbf * nbf, vmax = n2 / 2 + 1;
+    ctx->invalidate_all();
+    ctx->L_set = false;
+    ctx->L_gen = false;
+    std::vector<double> hcol((size_t)n2);
+    if (mshqc_ao_eri_diagonal(basis, hcol.data()) != MSHQC_AO_OK)
+        return set_error(MSHQC_CD_ERR_ARG, std::string("ERI diagonal: ") + mshqc_ao_last_error());
+    CD_ALLOC(ctx->scratch, sizeof(double) * (size_t)(n2 + 2), false);
+    double* D = ctx->scratch.as<double>();
+    double* pv = D + n2;
+    CD_RC(upload(ctx, D, hcol.data(), sizeof(double) * (size_t)n2));
+    CD_ALLOC(ctx->L, sizeof(double) * (size_t)(vmax * n2), false);
+    double* L = ctx->L.as<double>();
+    const unsigned blocks = (unsigned)cdiv(n2, 256);
+    int64_t m = 0;
+    bool conv = false;
+    for (; m < vmax; ++m) {
+        argmax_first_kernel<<<1, 1024, 0, ctx->stream>>>(D, n2, reinterpret_cast<int64_t*>(pv), pv + 1);
+        CD_CUDA(cudaGetLastError());
+        struct {
+            int64_t p;
+            double v;
+        } h;
+        CD_CUDA(cudaMemcpyAsync(&h, pv, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        CD_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (h.v < threshold) {   // also a negative largest diagonal
+            conv = h.v >= -1e-10;
+            break;
+        }
+        if (mshqc_ao_eri_column(basis, h.p, hcol.data()) != MSHQC_AO_OK)
+            return set_error(MSHQC_CD_ERR_ARG, std::string("ERI column: ") + mshqc_ao_last_error());
+        CD_RC(upload(ctx, L + m * n2, hcol.data(), sizeof(double) * (size_t)n2));
+        chol_direct_column_kernel<<<blocks, 256, 0, ctx->stream>>>(L, (int)m, n2, h.p, h.v, L + m * n2);
+        chol_direct_diag_update_kernel<<<blocks, 256, 0, ctx->stream>>>(D, L + m * n2, n2);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches += 3;
+    }
+    *n_vectors = m;
+    if (converged) *converged = conv ? 1 : 0;
     if (L_out) {
         if (m > max_vectors)
             return set_error(MSHQC_CD_ERR_ARG, "L_out holds " + std::to_string(max_vectors) + " vectors, " +

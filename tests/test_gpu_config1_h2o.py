@@ -49,3 +49,34 @@ def test_config1_h2o_ccpvdz_against_reference_cdrmp2():
     assert M == r["n_vectors"]
     assert abs(e64 - r["e_corr"]) <= 1e-9
     assert abs(e3 - r["e_corr"]) <= 1e-6
+
+
+def test_config1_integral_direct_decomposition():
+    """The integral-direct decomposition (mshqc_cd_cholesky_direct: ERI
+    diagonal and columns from the host engine, the vectors on the GPU, the
+    reference's DirectCholesky of src/integrals/cholesky_direct.cc) against the
+    decomposition of the full ERI tensor: the same pivots, hence the same
+    vectors to rounding, and the same CD-RMP2 energy to 1e-10 Eh."""
+    fix = json.load(open(os.path.join(HERE, "golden", "h2o_basis_sets.json")))
+    case = fix["cases"]["mshqc_h2o_ccpvdz"]
+    mol = ao.Molecule.from_angstrom(case["atoms"], case["angstrom_to_bohr"])
+    bs = ao.BasisSet.from_g94(fix["basis"]["cc-pvdz"]["g94"], mol)
+    eng = ao.IntegralEngine(mol, bs)
+    g = eng.compute_eri()
+    S, T, V = eng.compute_overlap(), eng.compute_kinetic(), eng.compute_nuclear()
+    s, U = np.linalg.eigh(S)
+    X = U @ np.diag(s ** -0.5) @ U.T
+    e, C = np.linalg.eigh(X.T @ (T + V) @ X)
+    C = X @ C                                     # core-Hamiltonian orbitals suffice here
+    with capi.Context(0) as ctx:
+        Lf = ctx.cholesky_decompose(g, 1e-6)
+        ctx.set_orbitals(capi.ALPHA, C, e, 5)
+        ef = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)["total"]
+        Ld = ctx.cholesky_direct(bs, 1e-6)
+        ctx.set_orbitals(capi.ALPHA, C, e, 5)
+        ed = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)["total"]
+    print(f"\nintegral-direct: {Ld.shape[0]} vectors (full tensor: {Lf.shape[0]}), max |dL| "
+          f"{np.max(np.abs(Ld - Lf)):.2e}, energy difference {abs(ed - ef):.2e} Eh")
+    assert Ld.shape == Lf.shape
+    assert np.max(np.abs(Ld - Lf)) <= 1e-10
+    assert abs(ed - ef) <= 1e-10
