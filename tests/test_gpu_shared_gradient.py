@@ -4,9 +4,11 @@ shares summed by shard.allreduce_gradient): two gloo processes on one GPU
 (their kernels never wait on each other; the collectives are staged through
 host memory), restricted and unrestricted, mixed precision and FP64.  The
 all-reduced energy and derivatives equal the unpartitioned gradient of the
-same process (1e-12 of the largest entry on the FP64 path, 1e-8 on the mixed
-path whose int8-slice transforms scale each share's operands by its own row
-maxima).  A one-rank NCCL group drives the NCCL callbacks of
+same process (1e-12 of the largest entry on the FP64 path; 2e-6 on the mixed
+path, whose shares run smaller occupied blocks than the whole gradient: Gamma,
+BF16x3 products accumulated in FP32 chunks per block pair, then rounds
+differently at ~1e-7 relative, and the int8-slice transforms scale each
+share's operands by its own row maxima).  A one-rank NCCL group drives the NCCL callbacks of
 shard.nccl_collectives on a library-sized buffer in place."""
 import os
 import socket
@@ -83,7 +85,7 @@ def test_two_ranks_share_transforms_and_backward():
         p.join(timeout=120)
         assert p.exitcode == 0
     for (kind_name, prec), (et, ef, ta, fa, tda, fda, tb, fb, eshare) in res.items():
-        tol = 1e-12 if prec == 0 else 1e-8
+        tol = 1e-12 if prec == 0 else 2e-6
         assert eshare != 0.0
         assert abs(et - ef) <= 1e-12 * abs(ef), (kind_name, prec)
         assert np.max(np.abs(ta - fa)) <= tol * np.max(np.abs(fa)), (kind_name, prec)
