@@ -132,6 +132,9 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
     amp_detail::local_pair(p, lp, ii, jj);
     const double wgt = p.tri ? (ii < jj ? 2.0 : 1.0) : p.wgt;
     const bool write_t = p.Thi != nullptr && !(p.tri && ii == jj);
+    // FP64 operand of a diagonal block pair: the (j, i) amplitudes go into A64
+    // as the transposes of the (i, j) ones
+    const bool write_t64 = !SPLIT && p.tri && ii != jj;
     const int xb0 = ch * ta / R, xb1 = (ch + 1) * ta / R;   // this CTA's row tiles
     const int i = p.i0 + ii, j = p.j0 + jj;
     const long long pair = (long long)i * p.oy + j;          // over all occupied rows
@@ -231,6 +234,13 @@ __global__ void __launch_bounds__(256, 4) amp_elem_kernel(AmpElemArgs p) {
 #pragma unroll
                     for (int e = 0; e < 8; ++e) col[e] = T[g * 8 + e][r];
                     amp_detail::store_hilo8(col, p.Thi + off, p.Tlo + off);
+                }
+            }
+            if (write_t64) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int rb = ty + 8 * k;   // b offset: row (j, b) of the operand
+                    p.A64[((long long)jj * p.ksy + b0 + rb) * p.ldA + (long long)ii * p.rsx + a0 + tx] = T[tx][rb];
                 }
             }
             if (pcol && ty == 0) {

@@ -86,6 +86,7 @@ struct mshqc_cd_ctx {
     mshqc_cd::DevBuf pair_sum;      // per-pair energies
     mshqc_cd::DevBuf totals;        // scalar results
     mshqc_cd::DevBuf flag;          // error / NaN flags
+    mshqc_cd::DevBuf pace;          // wave-pacing progress counters of the persistent tile kernels
     mshqc_cd::DevBuf amp;           // backward: staged amplitudes
     mshqc_cd::DevBuf gam[2];        // backward: Gamma per spin
     mshqc_cd::DevBuf BT;            // backward: transposed MO vectors (hi/lo BF16), alpha
@@ -155,6 +156,7 @@ struct mshqc_cd_ctx {
         pair_sum.release();
         totals.release();
         flag.release();
+        pace.release();
         amp.release();
         BT.release();
         amp2.release();

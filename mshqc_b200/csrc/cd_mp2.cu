@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -15,7 +16,6 @@
 #include "pair_energy_f64.cuh"
 #include "pair_energy_tc.cuh"
 #include "split_bf16.cuh"
-#include "backward_f64.cuh"
 #include "gamma_tc.cuh"
 #include "vtile_tc.cuh"
 #include "amp_elem.cuh"
@@ -54,11 +54,31 @@ bool owns_next(mshqc_cd_ctx* ctx) {
 // function of the problem dimensions and the number of ranks only, so that
 // every rank enumerates the same units whatever memory its GPU has free: at
 // most the staging these fixed budgets hold, and small enough that there are
-// about 32 units per rank for the cost-balanced plan (or 4 per rank for the
-// FP64 passes, whose units are blocks of rows).  MSHQC_CD_BWD_BLOCK (occupied
-// orbitals per block) overrides both rules in every pass.
+// about 32 units per rank for the cost-balanced plan (4 per rank in the
+// opposite-spin passes, whose units are blocks of rows against all columns).
+// MSHQC_CD_BWD_BLOCK (occupied orbitals per block) overrides both rules in
+// every pass.
 constexpr size_t kPartTcBudget = size_t(16) << 30;
-constexpr size_t kPartF64Budget = size_t(4) << 30;
+constexpr size_t kPartF64Budget = size_t(8) << 30;
+
+// Wave pacing of the persistent tile kernels (WavePacer in sm100_ptx.cuh):
+// copies per epoch and epochs of slack; MSHQC_CD_PACE=off disables it,
+// MSHQC_CD_PACE=<every>,<slack> sets both.
+void pace_params(int* every, int* slack) {
+    *every = 8;
+    *slack = 2;
+    const char* env = std::getenv("MSHQC_CD_PACE");
+    if (!env) return;
+    if (std::strcmp(env, "off") == 0) {
+        *every = 0;
+        return;
+    }
+    int e = 0, s = 0;
+    if (std::sscanf(env, "%d,%d", &e, &s) == 2 && e > 0 && s >= 0) {
+        *every = e;
+        *slack = s;
+    }
+}
 
 int64_t env_block() {
     const char* env = std::getenv("MSHQC_CD_BWD_BLOCK");
@@ -90,14 +110,25 @@ void tc_block_sizes(const mshqc_cd_ctx* ctx, int64_t ox, int64_t oy, int64_t VRx
     *bJ = sym ? *bI : oy;
 }
 
-// rows per block of an FP64 pass with per_i staging bytes per occupied row
-int64_t f64_block_rows(const mshqc_cd_ctx* ctx, int64_t ox, size_t per_i, size_t free_budget, size_t part_budget) {
+// block sizes (rows bI, columns bJ) of an FP64 pass: staging of S and of the
+// amplitudes, both FP64, per (i, j)
+void f64_block_sizes(const mshqc_cd_ctx* ctx, int64_t ox, int64_t oy, int64_t vpx, int64_t vpy, bool sym,
+                     size_t free_budget, int64_t* bI, int64_t* bJ) {
     const bool part = ctx->part_active;
-    const size_t budget = std::max<size_t>(per_i, part ? part_budget : free_budget);
-    int64_t bi = std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)(budget / per_i)));
-    if (part) bi = std::min<int64_t>(bi, std::max<int64_t>(1, cdiv(ox, 4 * (int64_t)ctx->part_size)));
-    if (const int64_t b = env_block()) bi = std::min<int64_t>(ox, b);
-    return bi;
+    const double budget = (double)(part ? kPartF64Budget : free_budget);
+    const double per_ij = 2.0 * sizeof(double) * (double)vpx * (double)vpy;
+    if (sym) {
+        *bI = std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)std::sqrt(budget / per_ij)));
+        if (part) {
+            const int64_t nb = (int64_t)std::ceil(std::sqrt(64.0 * ctx->part_size));
+            *bI = std::min<int64_t>(*bI, std::max<int64_t>(1, cdiv(ox, nb)));
+        }
+    } else {
+        *bI = std::max<int64_t>(1, std::min<int64_t>(ox, (int64_t)(budget / (per_ij * oy))));
+        if (part) *bI = std::min<int64_t>(*bI, std::max<int64_t>(1, cdiv(ox, 4 * (int64_t)ctx->part_size)));
+    }
+    if (const int64_t b = env_block()) *bI = std::min<int64_t>(ox, b);
+    *bJ = sym ? *bI : oy;
 }
 
 int require_inputs(mshqc_cd_ctx* ctx, int spin) {
@@ -925,72 +956,6 @@ int transposed_dispatch(mshqc_cd_ctx* ctx, int spin, double scale, double* dC, i
     return transposed_transforms(ctx, spin, scale, dC);
 }
 
-// Restricted FP64 gradient: amplitude pass + Gamma GEMM per block of occupied
-// rows, then the transposed half transforms.  dC (column-major N*N, device),
-// deps (N, device) are written; *energy gets the closed-shell E.
-int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
-    SpinState& s = ctx->spin[0];
-    const int64_t N = ctx->N, Mp = ctx->Mp, o = s.nocc, v = N - o, vp = s.vp;
-    const int nb = (int)(vp / 64);
-    // occupied block size for the amplitude staging buffer
-    size_t free_b = 0, total_b = 0;
-    CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_i = sizeof(double) * (size_t)vp * o * vp;
-    const int bi = (int)f64_block_rows(ctx, o, per_i, std::min<size_t>(free_b / 4, size_t(16) << 30),
-                                       kPartF64Budget);
-    CD_ALLOC(ctx->amp, per_i * bi, false);
-    // zeroed: with a partition the blocks of other ranks stay zero
-    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)b_rows(ctx, o) * vp * Mp, ctx->part_active);
-    CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
-    const int64_t units_per_i = (int64_t)o * nb * nb;
-    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * units_per_i), ctx->part_active);
-    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
-    const size_t smem = pair_f64_detail::SMEM_BYTES;
-    CD_CUDA(cudaFuncSetAttribute(amp_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    for (int i0 = 0; i0 < o; i0 += bi) {
-        if (!owns_next(ctx)) continue;
-        const int nbi = (int)std::min<int64_t>(bi, o - i0);
-        AmpF64Args a{};
-        a.X = s.B64.as<double>();
-        a.o = (int)o;  a.v = (int)v;  a.vp = (int)vp;  a.Mp = (int)Mp;
-        a.i0 = i0;  a.bi = nbi;
-        a.eo = s.eps.as<double>();  a.ev = a.eo + o;
-        a.amp = ctx->amp.as<double>();
-        a.deps = deps;
-        a.partial = ctx->partial.as<double>() + (int64_t)i0 * units_per_i;
-        a.nb = nb;
-        const int64_t units = (int64_t)nbi * units_per_i;
-        begin_stage(ctx, ST_AMPLITUDE);
-        amp_f64_kernel<<<(unsigned)units, 256, smem, ctx->stream>>>(a);
-        end_stage(ctx);
-        CD_CUDA(cudaGetLastError());
-        ctx->launches++;
-        // Gamma[(i,a)][Q] = sum_{(j,b)} tt[(i,a)][(j,b)] B[(j,b)][Q]
-        GemmF64Args g{};
-        g.M = (int)(nbi * vp);  g.N = (int)Mp;  g.K = (int)(o * vp);  g.batch = 1;
-        g.A = ctx->amp.as<double>();  g.lda = o * vp;  g.sA = 0;
-        g.B = s.B64.as<double>();  g.ldb = Mp;  g.sB = 0;
-        g.C = ctx->gam[0].as<double>() + (int64_t)i0 * vp * Mp;  g.ldc = Mp;  g.sC = 0;
-        g.alpha = 1.0;  g.beta = 0.0;
-        begin_stage(ctx, ST_GAMMA);
-        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
-        end_stage(ctx);
-        ctx->launches++;
-    }
-    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * units_per_i),
-                                                   ctx->totals.as<double>());
-    CD_CUDA(cudaGetLastError());
-    ctx->launches++;
-    CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-
-    begin_stage(ctx, ST_TRANSPOSED);
-    CD_RC(transposed_transforms(ctx, 0, 4.0, dC));
-    end_stage(ctx);
-    CD_CUDA(cudaStreamSynchronize(ctx->stream));
-    return MSHQC_CD_OK;
-}
-
-
 // ---------------------------------------------------------------------------
 // backward building blocks (tensor-core and FP64 unrestricted passes)
 // ---------------------------------------------------------------------------
@@ -1052,6 +1017,13 @@ int launch_gamma(mshqc_cd_ctx* ctx, const uint16_t* ahi, const uint16_t* alo, in
     const size_t gsm = gamma_tc::SMEM_BYTES;
     CD_CUDA(cudaFuncSetAttribute(gamma_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
     const int grid = (int)std::min<int64_t>((int64_t)g.nrb * g.nqb, ctx->num_sms);
+    g.group = 16;
+    if (const char* env = std::getenv("MSHQC_CD_GAMMA_GROUP")) g.group = std::max(1, std::atoi(env));
+    pace_params(&g.pace_every, &g.pace_slack);
+    if (g.pace_every > 0) {
+        CD_ALLOC(ctx->pace, sizeof(int) * (size_t)grid, true);
+        g.pace = ctx->pace.as<int>();
+    }
     begin_stage(ctx, ST_GAMMA);
     gamma_tc_kernel<<<grid, gamma_tc::THREADS, gsm, ctx->stream>>>(g);
     end_stage(ctx);
@@ -1145,6 +1117,11 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             a.tri = tri ? 1 : 0;
             const int64_t vunits = (int64_t)npl * a.nbx * a.nby;
             const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
+            pace_params(&a.pace_every, &a.pace_slack);
+            if (a.pace_every > 0) {
+                CD_ALLOC(ctx->pace, sizeof(int) * (size_t)vgrid, true);
+                a.pace = ctx->pace.as<int>();
+            }
             begin_stage(ctx, ST_AMPLITUDE);
             vtile_tc_kernel<<<vgrid, vtile_tc::THREADS, vsm, ctx->stream>>>(a);
             end_stage(ctx);
@@ -1174,7 +1151,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             // pair alone does not fill the GPU several times over
             const int ta = (int)(dx.VR / 32);
             int nch = 1;
-            while (nch < 4 && 2 * nch <= ta && (int64_t)npl * nch < 8LL * ctx->num_sms) nch *= 2;
+            while (nch < 16 && 2 * nch <= ta && (int64_t)npl * nch < 8LL * ctx->num_sms) nch *= 2;
             e.nchunk = nch;
             if (nch > 1) {
                 const size_t per = (size_t)npl * nch;
@@ -1211,82 +1188,139 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
     return MSHQC_CD_OK;
 }
 
-// The FP64 counterpart: S = B_x(block) B_y^T and the Gamma products as FP64
-// DMMA GEMMs around the same element-wise pass.
+// The FP64 counterpart of tc_backward_pass, over the same block pairs: S =
+// B_x[I] B_y[J]^T and the Gamma products as FP64 DMMA GEMMs around the
+// element-wise pass.  A diagonal block pair of the symmetric modes forms S
+// for j >= i only (one GEMM per row i), and the element-wise pass completes
+// the amplitude block with the transposes.
 template <int MODE>
 int f64_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, double* deps_x, double* deps_y, double* partial) {
+    constexpr bool kSym = MODE != AMP_OPPOSITE_SPIN;
     SpinState& X = ctx->spin[sx];
     SpinState& Y = ctx->spin[sy];
     const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
-    const int64_t Mp = ctx->Mp, ldS = dy.o * dy.vp;
+    const int64_t Mp = ctx->Mp;
     size_t free_b = 0, total_b = 0;
     CD_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_i = 2 * sizeof(double) * (size_t)dx.vp * ldS;
-    const int bi = (int)f64_block_rows(ctx, dx.o, per_i, std::min<size_t>(free_b / 4, size_t(32) << 30),
-                                       2 * kPartF64Budget);
-    CD_ALLOC(ctx->W, per_i / 2 * bi, false);
-    CD_ALLOC(ctx->amp, per_i / 2 * bi, false);
+    const size_t held = ctx->amp.bytes + ctx->W.bytes;
+    const size_t budget = std::min<size_t>((free_b + held) / 3, size_t(40) << 30);
+    int64_t bI, bJ;
+    f64_block_sizes(ctx, dx.o, dy.o, dx.vp, dy.vp, kSym, budget, &bI, &bJ);
+    const size_t n_stage = sizeof(double) * (size_t)(bI * dx.vp) * (size_t)(bJ * dy.vp);
+    CD_ALLOC(ctx->W, n_stage, false);
+    CD_ALLOC(ctx->amp, n_stage, false);
     const int64_t npairs = dx.o * dy.o;
-    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.vp + dy.vp + 1)), ctx->part_active);
-    if (ctx->part_active) CD_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * (size_t)npairs, ctx->stream));
+    CD_ALLOC(ctx->dsum, sizeof(double) * (size_t)(npairs * (dx.vp + dy.vp + 1)), true);
+    CD_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * (size_t)npairs, ctx->stream));
     double* prow = ctx->dsum.as<double>();
     double* pcol = prow + npairs * dx.vp;
     double* pocc = pcol + npairs * dy.vp;
-    for (int i0 = 0; i0 < dx.o; i0 += bi) {
-        if (!owns_next(ctx)) continue;
-        const int nbi = (int)std::min<int64_t>(bi, dx.o - i0);
-        const double* Xb = X.B64.as<double>() + (int64_t)i0 * dx.vp * Mp;
-        // S[(i,a)][(j,b)] = sum_Q X[(i,a)][Q] Y[(j,b)][Q]
-        GemmF64Args g{};
-        g.M = (int)(nbi * dx.vp);  g.N = (int)ldS;  g.K = (int)Mp;  g.batch = 1;
-        g.A = Xb;  g.lda = Mp;  g.sA = 0;
-        g.B = Y.B64.as<double>();  g.ldb = Mp;  g.sB = 0;
-        g.C = ctx->W.as<double>();  g.ldc = ldS;  g.sC = 0;
-        g.alpha = 1.0;  g.beta = 0.0;
-        begin_stage(ctx, ST_AMPLITUDE);
-        CD_CUDA(gemm_f64(g, true, true, ctx->stream));
-        end_stage(ctx);
-        ctx->launches++;
-        AmpElemArgs e{};
-        e.S = ctx->W.as<double>();
-        e.ldS = ldS;
-        e.rsx = (int)dx.vp;  e.csy = (int)dy.vp;  e.ksy = (int)dy.vp;
-        e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
-        e.i0 = i0;  e.nbi = nbi;  e.j0 = 0;  e.nbj = (int)dy.o;  e.wgt = 1.0;
-        e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
-        e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
-        e.A64 = ctx->amp.as<double>();  e.ldA = ldS;
-        e.partial = partial;
-        e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
-        begin_stage(ctx, ST_AMP_ELEM);
-        amp_elem_kernel<MODE, false><<<(unsigned)(nbi * dy.o), 256, 0, ctx->stream>>>(e);
-        end_stage(ctx);
-        CD_CUDA(cudaGetLastError());
-        ctx->launches++;
-        begin_stage(ctx, ST_GAMMA);
-        // Gamma_x[(i,a)][Q] += sum_{(j,b)} t[(i,a)][(j,b)] Y[(j,b)][Q]
-        GemmF64Args h{};
-        h.M = (int)(nbi * dx.vp);  h.N = (int)Mp;  h.K = (int)ldS;  h.batch = 1;
-        h.A = ctx->amp.as<double>();  h.lda = ldS;  h.sA = 0;
-        h.B = Y.B64.as<double>();  h.ldb = Mp;  h.sB = 0;
-        h.C = ctx->gam[sx].as<double>() + (int64_t)i0 * dx.vp * Mp;  h.ldc = Mp;  h.sC = 0;
-        h.alpha = 1.0;  h.beta = 1.0;
-        CD_CUDA(gemm_f64(h, true, false, ctx->stream));
-        ctx->launches++;
-        if (MODE == AMP_OPPOSITE_SPIN) {
-            // Gamma_y[(j,b)][Q] += sum_{(i,a) in block} t[(i,a)][(j,b)] X[(i,a)][Q]
-            GemmF64Args k{};
-            k.M = (int)ldS;  k.N = (int)Mp;  k.K = (int)(nbi * dx.vp);  k.batch = 1;
-            k.A = ctx->amp.as<double>();  k.lda = ldS;  k.sA = 0;
-            k.B = Xb;  k.ldb = Mp;  k.sB = 0;
-            k.C = ctx->gam[sy].as<double>();  k.ldc = Mp;  k.sC = 0;
-            k.alpha = 1.0;  k.beta = 1.0;
-            CD_CUDA(gemm_f64(k, false, false, ctx->stream));
+    double* S = ctx->W.as<double>();
+    double* A = ctx->amp.as<double>();
+    for (int64_t I0 = 0; I0 < dx.o; I0 += bI) {
+        const int nI = (int)std::min<int64_t>(bI, dx.o - I0);
+        const double* XI = X.B64.as<double>() + I0 * dx.vp * Mp;
+        for (int64_t J0 = kSym ? I0 : 0; J0 < dy.o; J0 += bJ) {
+            if (!owns_next(ctx)) continue;
+            const int nJ = (int)std::min<int64_t>(bJ, dy.o - J0);
+            const bool mirror = !kSym || J0 != I0;
+            const bool tri = kSym && J0 == I0;
+            const int npl = tri ? nI * (nI + 1) / 2 : nI * nJ;
+            const int64_t ldS = (int64_t)nJ * dy.vp;
+            const double* YJ = Y.B64.as<double>() + J0 * dy.vp * Mp;
+            // S[(i,a)][(j,b)] = sum_Q X[(i,a)][Q] Y[(j,b)][Q]
+            begin_stage(ctx, ST_AMPLITUDE);
+            for (int r = 0; r < (tri ? nI : 1); ++r) {
+                GemmF64Args g{};
+                g.M = (int)((tri ? 1 : nI) * dx.vp);  g.N = (int)((nJ - r) * dy.vp);  g.K = (int)Mp;  g.batch = 1;
+                g.A = XI + (int64_t)r * dx.vp * Mp;  g.lda = Mp;  g.sA = 0;
+                g.B = YJ + (int64_t)r * dy.vp * Mp;  g.ldb = Mp;  g.sB = 0;
+                g.C = S + (int64_t)r * dx.vp * ldS + (int64_t)r * dy.vp;  g.ldc = ldS;  g.sC = 0;
+                g.alpha = 1.0;  g.beta = 0.0;
+                CD_CUDA(gemm_f64(g, true, true, ctx->stream));
+                ctx->launches++;
+            }
+            end_stage(ctx);
+            AmpElemArgs e{};
+            e.S = S;
+            e.ldS = ldS;
+            e.rsx = (int)dx.vp;  e.csy = (int)dy.vp;  e.ksy = (int)dy.vp;
+            e.ox = (int)dx.o;  e.oy = (int)dy.o;  e.vx = (int)dx.v;  e.vy = (int)dy.v;
+            e.i0 = (int)I0;  e.nbi = nI;  e.j0 = (int)J0;  e.nbj = nJ;
+            e.wgt = (kSym && mirror) ? 2.0 : 1.0;
+            e.tri = tri ? 1 : 0;
+            e.eox = X.eps.as<double>();  e.evx = e.eox + dx.o;
+            e.eoy = Y.eps.as<double>();  e.evy = e.eoy + dy.o;
+            e.A64 = A;  e.ldA = ldS;
+            e.partial = partial;
+            e.prow = prow;  e.pcol = pcol;  e.pocc = pocc;
+            const int ta = (int)(dx.vp / 32);
+            int nch = 1;
+            while (nch < 16 && 2 * nch <= ta && (int64_t)npl * nch < 8LL * ctx->num_sms) nch *= 2;
+            e.nchunk = nch;
+            if (nch > 1) {
+                const size_t per = (size_t)npl * nch;
+                CD_ALLOC(ctx->amp_chunks, sizeof(double) * per * ((size_t)dy.vp + 2), false);
+                e.cpcol = ctx->amp_chunks.as<double>();
+                e.cpart = e.cpcol + per * dy.vp;
+                e.cpocc = e.cpart + per;
+            }
+            begin_stage(ctx, ST_AMP_ELEM);
+            amp_elem_kernel<MODE, false><<<(unsigned)(npl * nch), 256, 0, ctx->stream>>>(e);
+            CD_CUDA(cudaGetLastError());
             ctx->launches++;
+            if (nch > 1) {
+                amp_chunks_combine_kernel<<<(unsigned)cdiv((int64_t)npl * dy.vp, 256), 256, 0, ctx->stream>>>(e, npl);
+                CD_CUDA(cudaGetLastError());
+                ctx->launches++;
+            }
+            end_stage(ctx);
+            begin_stage(ctx, ST_GAMMA);
+            // Gamma_x[(i,a)][Q] += sum_{(j,b) in J} t[(i,a)][(j,b)] Y[(j,b)][Q]
+            GemmF64Args h{};
+            h.M = (int)(nI * dx.vp);  h.N = (int)Mp;  h.K = (int)ldS;  h.batch = 1;
+            h.A = A;  h.lda = ldS;  h.sA = 0;
+            h.B = YJ;  h.ldb = Mp;  h.sB = 0;
+            h.C = ctx->gam[sx].as<double>() + I0 * dx.vp * Mp;  h.ldc = Mp;  h.sC = 0;
+            h.alpha = 1.0;  h.beta = 1.0;
+            CD_CUDA(gemm_f64(h, true, false, ctx->stream));
+            ctx->launches++;
+            if (mirror) {
+                // Gamma_y[(j,b)][Q] += sum_{(i,a) in I} t[(i,a)][(j,b)] X[(i,a)][Q]
+                GemmF64Args k{};
+                k.M = (int)ldS;  k.N = (int)Mp;  k.K = (int)(nI * dx.vp);  k.batch = 1;
+                k.A = A;  k.lda = ldS;  k.sA = 0;
+                k.B = XI;  k.ldb = Mp;  k.sB = 0;
+                k.C = ctx->gam[sy].as<double>() + J0 * dy.vp * Mp;  k.ldc = Mp;  k.sC = 0;
+                k.alpha = 1.0;  k.beta = 1.0;
+                CD_CUDA(gemm_f64(k, false, false, ctx->stream));
+                ctx->launches++;
+            }
+            end_stage(ctx);
         }
-        end_stage(ctx);
     }
     CD_RC(reduce_deps(ctx, prow, pcol, pocc, dx.o, dy.o, dx.vp, dy.vp, dx.v, dy.v, deps_x, deps_y));
+    return MSHQC_CD_OK;
+}
+
+// Restricted FP64 gradient: one FP64 block-pair pass, then the transposed
+// half transforms with dE/dB = 4 Gamma.
+int gradient_restricted_f64(mshqc_cd_ctx* ctx, double* dC, double* deps, double* energy) {
+    SpinState& s = ctx->spin[0];
+    const int64_t N = ctx->N, Mp = ctx->Mp, o = s.nocc;
+    CD_ALLOC(ctx->gam[0], sizeof(double) * (size_t)b_rows(ctx, o) * s.vp * Mp, true);
+    CD_CUDA(cudaMemsetAsync(deps, 0, sizeof(double) * N, ctx->stream));
+    CD_ALLOC(ctx->totals, sizeof(double) * 8, false);
+    CD_ALLOC(ctx->partial, sizeof(double) * (size_t)(o * o), false);
+    CD_RC(f64_backward_pass<AMP_RESTRICTED>(ctx, 0, 0, deps, deps, ctx->partial.as<double>()));
+    reduce_total_kernel<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), (int)(o * o), ctx->totals.as<double>());
+    CD_CUDA(cudaGetLastError());
+    ctx->launches++;
+    CD_CUDA(cudaMemcpyAsync(energy, ctx->totals.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    begin_stage(ctx, ST_TRANSPOSED);
+    CD_RC(transposed_dispatch(ctx, 0, 4.0, dC, MSHQC_CD_FP64));
+    end_stage(ctx);
     return MSHQC_CD_OK;
 }
 
@@ -1401,18 +1435,25 @@ int plan_partition(mshqc_cd_ctx* ctx, int kind, int precision) {
             }
         }
     };
-    auto f64_pass = [&](int sx, int sy, bool os) {
+    // the FP64 passes visit the same kind of units; per block pair: S GEMM
+    // (half of it on a diagonal block pair) + Gamma products
+    auto f64_pass = [&](int sx, int sy, bool sym) {
         const BwdDims dx = bwd_dims(ctx, sx), dy = bwd_dims(ctx, sy);
-        const size_t per_i = 2 * sizeof(double) * (size_t)dx.vp * (size_t)(dy.o * dy.vp);
-        const int64_t bi = f64_block_rows(ctx, dx.o, per_i, 0, 2 * kPartF64Budget);
-        for (int64_t i0 = 0; i0 < dx.o; i0 += bi)
-            cost.push_back((double)std::min(bi, dx.o - i0) * dy.o * (os ? 3.0 : 2.0));
+        int64_t bI, bJ;
+        f64_block_sizes(ctx, dx.o, dy.o, dx.vp, dy.vp, sym, 0, &bI, &bJ);
+        for (int64_t I0 = 0; I0 < dx.o; I0 += bI) {
+            const int64_t nI = std::min(bI, dx.o - I0);
+            for (int64_t J0 = sym ? I0 : 0; J0 < dy.o; J0 += bJ) {
+                const int64_t nJ = std::min(bJ, dy.o - J0);
+                if (sym && J0 == I0)
+                    cost.push_back(0.5 * (double)nI * (nI + 1) + (double)nI * nI);
+                else
+                    cost.push_back(3.0 * nI * nJ);
+            }
+        }
     };
     if (!unres && precision == MSHQC_CD_FP64) {
-        const BwdDims d = bwd_dims(ctx, 0);
-        const size_t per_i = sizeof(double) * (size_t)d.vp * d.o * d.vp;
-        const int64_t bi = f64_block_rows(ctx, d.o, per_i, 0, kPartF64Budget);
-        for (int64_t i0 = 0; i0 < d.o; i0 += bi) cost.push_back((double)std::min(bi, d.o - i0));
+        f64_pass(0, 0, true);
     } else if (!unres) {
         tc_pass(0, 0, true);
     } else if (precision == MSHQC_CD_FP16X3) {
@@ -1420,9 +1461,9 @@ int plan_partition(mshqc_cd_ctx* ctx, int kind, int precision) {
         tc_pass(1, 1, true);
         tc_pass(0, 1, false);
     } else {
-        f64_pass(0, 0, false);
-        f64_pass(1, 1, false);
-        f64_pass(0, 1, true);
+        f64_pass(0, 0, true);
+        f64_pass(1, 1, true);
+        f64_pass(0, 1, false);
     }
     std::vector<size_t> order(cost.size());
     for (size_t k = 0; k < order.size(); ++k) order[k] = k;

@@ -44,6 +44,9 @@ struct GammaTcArgs {
     double* gamma;          // [o][vp][Mp]
     int accumulate;         // 1: gamma += result, 0: gamma = result
     int* err;
+    int* pace;              // gridDim.x zeroed progress counters (WavePacer), or null
+    int pace_every, pace_slack;
+    int group;              // row blocks per tile group (>= 1), see gamma_tile
 };
 
 namespace gamma_tc {
@@ -55,8 +58,22 @@ constexpr uint32_t STAGE_BYTES = KS * 2 * (SLAB_A + SLAB_B);   // 48 KB: KS step
 constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;           // 192 KB
 constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 + 256;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
+constexpr uint64_t kPaceLimitNs = 200000ull;   // a pacing wait longer than this turns pacing off
 constexpr uint32_t TMEM_COLS = 512;
 }  // namespace gamma_tc
+
+// Tile u -> (row block rb, Q block qb).  Tiles come in groups of `group` row
+// blocks with all Q blocks, Q-block-major inside a group, so the 148 tiles of
+// one wave (consecutive u) span about `group` row blocks and 148 / group Q
+// blocks: the operand rows a wave reads, (group * 128 + 148 / group * 256)
+// per K step, are fewest near group = 16.  group = 1 is row-block-major.
+__device__ __forceinline__ void gamma_tile(const GammaTcArgs& p, long long u, long long& rb, long long& qb) {
+    const long long G = p.group, per = G * p.nqb, grp = u / per;
+    const long long g0 = grp * G, gsz = min((long long)p.nrb - g0, G);
+    const long long w = u - grp * per;
+    qb = w / gsz;
+    rb = g0 + w % gsz;
+}
 
 __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
     using namespace gamma_tc;
@@ -99,30 +116,47 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
     const int nchunks = (p.nk + p.KP - 1) / p.KP;
 
     if (warp == 0) {
-        if (lane == 0) {
-            uint32_t stage = 0, phase = 0;
-            uint32_t fill_phase = 0, filled = 0;   // bit s: parity / presence of stage s's last fill
-            for (long long u = first; u < units && !*abort_flag; u += step) {
-                const long long rb = u / p.nqb, qb = u % p.nqb;
-                const size_t ra0 = (size_t)rb * p.a_rbs * (BM * 16), rq0 = (size_t)qb * p.b_rbs * (BN * 16);
-                for (int kq = 0; kq < p.nk; kq += KS) {
-                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
+        // producer: lane 0 issues the copies, the whole warp paces
+        WavePacer pacer;
+        pacer.init(p.pace, (int)gridDim.x, p.pace_every, p.pace_slack);
+        uint32_t stage = 0, phase = 0;
+        uint32_t fill_phase = 0, filled = 0;   // bit s: parity / presence of stage s's last fill
+        bool stop = false;
+        for (long long u = first; u < units && !stop; u += step) {
+            long long rb, qb;
+            gamma_tile(p, u, rb, qb);
+            const size_t ra0 = (size_t)rb * p.a_rbs * (BM * 16), rq0 = (size_t)qb * p.b_rbs * (BN * 16);
+            for (int kq = 0; kq < p.nk; kq += KS) {
+                pacer.step(lane, kPaceLimitNs);
+                int ok = 1;
+                if (lane == 0) {
+                    if (*abort_flag) {
+                        ok = 0;
+                    } else if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
                         atomicExch(p.err, 11);
                         *abort_flag = 1;
-                        break;
+                        ok = 0;
+                    } else {
+                        uint8_t* sb = smem + stage * STAGE_BYTES;
+                        mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                        const size_t ka = ra0 + (size_t)kq * (BM * 16), kb = rq0 + (size_t)kq * (BN * 16);
+                        bulk_g2s(sb + OFF_AH, p.Ahi + ka, KS * SLAB_A, &full[stage]);
+                        bulk_g2s(sb + OFF_AL, p.Alo + ka, KS * SLAB_A, &full[stage]);
+                        bulk_g2s(sb + OFF_BH, p.Bhi + kb, KS * SLAB_B, &full[stage]);
+                        bulk_g2s(sb + OFF_BL, p.Blo + kb, KS * SLAB_B, &full[stage]);
                     }
-                    uint8_t* sb = smem + stage * STAGE_BYTES;
-                    mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-                    const size_t ka = ra0 + (size_t)kq * (BM * 16), kb = rq0 + (size_t)kq * (BN * 16);
-                    bulk_g2s(sb + OFF_AH, p.Ahi + ka, KS * SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_AL, p.Alo + ka, KS * SLAB_A, &full[stage]);
-                    bulk_g2s(sb + OFF_BH, p.Bhi + kb, KS * SLAB_B, &full[stage]);
-                    bulk_g2s(sb + OFF_BL, p.Blo + kb, KS * SLAB_B, &full[stage]);
-                    fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
-                    filled |= 1u << stage;
-                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    stop = true;
+                    break;
+                }
+                fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
+                filled |= 1u << stage;
+                if (++stage == STAGES) { stage = 0; phase ^= 1; }
             }
+        }
+        pacer.finish(lane);
+        if (lane == 0) {
             if (!*abort_flag) {
                 for (int s = 0; s < STAGES; ++s) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
@@ -215,21 +249,17 @@ __global__ void __launch_bounds__(576, 1) gamma_tc_kernel(GammaTcArgs p) {
             }
             if (!ok) break;
             // write this thread's row of the tile
-            const long long rb = u / p.nqb, qb = u % p.nqb;
+            long long rb, qb;
+            gamma_tile(p, u, rb, qb);
             const long long R = rb * BM + q * 32 + lane;
             const int i = p.i0 + (int)(R / p.VR), a = (int)(R % p.VR);
             if (a < p.v) {
-                double* dst = p.gamma + ((long long)i * p.vp + a) * p.Mp;
+                // Mp and q0 are multiples of 8 (16-byte aligned blocks of 8)
                 const int q0 = (int)(qb * BN) + part * 64;
-                if (p.accumulate) {
+                double* dst = p.gamma + ((long long)i * p.vp + a) * p.Mp + q0;
 #pragma unroll
-                    for (int c = 0; c < 64; ++c)
-                        if (q0 + c < p.Mp) dst[q0 + c] += (double)acc[c];
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 64; ++c)
-                        if (q0 + c < p.Mp) dst[q0 + c] = (double)acc[c];
-                }
+                for (int c = 0; c < 64; c += 8)
+                    if (q0 + c < p.Mp) f32x8_to_f64(dst + c, &acc[c], p.accumulate != 0);
             }
         }
     }

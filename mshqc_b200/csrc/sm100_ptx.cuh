@@ -54,6 +54,110 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
+// Relaxed GPU-scope loads and stores of an int shared between CTAs (progress
+// counters that order nothing the results depend on).
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(int* p, int v) {
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// dst[0..7] (+)= (double)src[0..7] as one ordered block of 16-byte accesses
+// (dst 16-byte aligned).  As inline PTX the compiler keeps the block in
+// place, so the 8 conversions of one block are live at a time instead of
+// being hoisted over a whole tile row.
+__device__ __forceinline__ void f32x8_to_f64(double* dst, const float* src, bool accumulate) {
+    if (accumulate)
+        asm volatile(
+            "{\n\t.reg .f64 x<8>, y<8>;\n\t"
+            "ld.global.v2.f64 {x0, x1}, [%0];\n\t"
+            "ld.global.v2.f64 {x2, x3}, [%0+16];\n\t"
+            "ld.global.v2.f64 {x4, x5}, [%0+32];\n\t"
+            "ld.global.v2.f64 {x6, x7}, [%0+48];\n\t"
+            "cvt.f64.f32 y0, %1;\n\tcvt.f64.f32 y1, %2;\n\tcvt.f64.f32 y2, %3;\n\tcvt.f64.f32 y3, %4;\n\t"
+            "cvt.f64.f32 y4, %5;\n\tcvt.f64.f32 y5, %6;\n\tcvt.f64.f32 y6, %7;\n\tcvt.f64.f32 y7, %8;\n\t"
+            "add.rn.f64 x0, x0, y0;\n\tadd.rn.f64 x1, x1, y1;\n\tadd.rn.f64 x2, x2, y2;\n\tadd.rn.f64 x3, x3, y3;\n\t"
+            "add.rn.f64 x4, x4, y4;\n\tadd.rn.f64 x5, x5, y5;\n\tadd.rn.f64 x6, x6, y6;\n\tadd.rn.f64 x7, x7, y7;\n\t"
+            "st.global.v2.f64 [%0], {x0, x1};\n\t"
+            "st.global.v2.f64 [%0+16], {x2, x3};\n\t"
+            "st.global.v2.f64 [%0+32], {x4, x5};\n\t"
+            "st.global.v2.f64 [%0+48], {x6, x7};\n\t"
+            "}\n" ::"l"(dst),
+            "f"(src[0]), "f"(src[1]), "f"(src[2]), "f"(src[3]), "f"(src[4]), "f"(src[5]), "f"(src[6]), "f"(src[7])
+            : "memory");
+    else
+        asm volatile(
+            "{\n\t.reg .f64 y<8>;\n\t"
+            "cvt.f64.f32 y0, %1;\n\tcvt.f64.f32 y1, %2;\n\tcvt.f64.f32 y2, %3;\n\tcvt.f64.f32 y3, %4;\n\t"
+            "cvt.f64.f32 y4, %5;\n\tcvt.f64.f32 y5, %6;\n\tcvt.f64.f32 y6, %7;\n\tcvt.f64.f32 y7, %8;\n\t"
+            "st.global.v2.f64 [%0], {y0, y1};\n\t"
+            "st.global.v2.f64 [%0+16], {y2, y3};\n\t"
+            "st.global.v2.f64 [%0+32], {y4, y5};\n\t"
+            "st.global.v2.f64 [%0+48], {y6, y7};\n\t"
+            "}\n" ::"l"(dst),
+            "f"(src[0]), "f"(src[1]), "f"(src[2]), "f"(src[3]), "f"(src[4]), "f"(src[5]), "f"(src[6]), "f"(src[7])
+            : "memory");
+}
+
+// Wave pacing of a persistent kernel whose CTAs share operands through L2.
+// The CTAs of one wave of tiles read the same operand slabs; if they stay
+// within a few microseconds of each other, every slab comes from DRAM once
+// and serves all of them from L2.  Left alone they drift apart, L2 evicts a
+// slab before its last reader arrives, the misses raise the DRAM fill rate
+// and shorten what L2 keeps, and the drift feeds itself.  The producer warp of
+// each CTA counts the copies it issues; every `every` copies it publishes
+// its epoch in prog[cta] and waits until every CTA has published at least
+// epoch - slack.  The slowest CTA's own condition always holds, so every wait
+// ends while all CTAs are resident; a wait that runs past limit_ns (a CTA not
+// resident because another kernel holds its SM) turns pacing off for the rest
+// of the launch.  Pacing orders no data the results depend on.  All 32 lanes
+// of the producer warp call step() together.
+struct WavePacer {
+    int* prog;
+    int ncta, every, slack, cnt;
+    bool on;
+    __device__ void init(int* p, int n, int ev, int sl) {
+        prog = p;
+        ncta = n;
+        every = ev > 0 ? ev : 1;
+        slack = sl;
+        cnt = 0;
+        on = p != nullptr;
+    }
+    __device__ void step(int lane, uint64_t limit_ns) {
+        if (!on) return;
+        if (cnt % every == 0) {
+            const int e = cnt / every;
+            if (lane == 0) st_relaxed_gpu(prog + blockIdx.x, e);
+            if (e > slack) {
+                const int target = e - slack;
+                uint64_t t0 = globaltimer_ns();
+                t0 = __shfl_sync(0xffffffffu, t0, 0);
+                while (true) {
+                    bool ok = true;
+                    for (int c = lane; c < ncta; c += 32) ok &= ld_relaxed_gpu(prog + c) >= target;
+                    if (__all_sync(0xffffffffu, ok)) break;
+                    uint64_t dt = globaltimer_ns() - t0;
+                    dt = __shfl_sync(0xffffffffu, dt, 0);
+                    if (dt > limit_ns) {
+                        on = false;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        ++cnt;
+    }
+    // this CTA issues no more copies: nobody waits for it
+    __device__ void finish(int lane) {
+        if (prog && lane == 0) st_relaxed_gpu(prog + blockIdx.x, 0x7fffffff);
+    }
+};
+
 // Named barrier `id` over `nthreads` threads that also returns whether ANY of
 // them passed pred = true, so a group of warps leaves a loop together.
 __device__ __forceinline__ bool bar_any(int id, int nthreads, bool pred) {

@@ -43,6 +43,8 @@ struct VtileArgs {
     float* S;               // staging [nbi * VR][nbj * VS]
     int* err;
     int tri;                // 1: only the pairs ii <= jj of a diagonal block (nbi == nbj)
+    int* pace;              // gridDim.x zeroed progress counters (WavePacer), or null
+    int pace_every, pace_slack;
 };
 
 // Local pair pr -> (ii, jj): row-major over nbi x nbj, or over the upper
@@ -71,6 +73,7 @@ constexpr uint32_t STAGE_BYTES = KS * 2 * (SLAB_A + SLAB_B);   // 48 KB
 constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;           // 192 KB
 constexpr size_t SMEM_BYTES = SMEM_DATA + 1024 + 256 + BN * 8;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
+constexpr uint64_t kPaceLimitNs = 200000ull;   // a pacing wait longer than this turns pacing off
 constexpr uint32_t TMEM_COLS = 512;
 }  // namespace vtile_tc
 
@@ -117,43 +120,59 @@ __global__ void __launch_bounds__(192, 1) vtile_tc_kernel(VtileArgs p) {
     const int nk = p.nqc;
 
     if (warp == 0) {
-        if (lane == 0) {
-            uint32_t stage = 0, phase = 0, fill_phase = 0, filled = 0;
-            for (long long u = first; u < units && !*abort_flag; u += step) {
-                const long long pr = u / per_pair, bb = u % per_pair;
-                int ii, jj;
-                vtile_pair(p, pr, ii, jj);
-                const int i = p.i0 + ii, j = p.j0 + jj;
-                const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
-                // slab bases at Q step 0 (256-row blocks of nqc steps, 4096 elements a step)
-                const size_t nq = (size_t)p.nqc;
-                const size_t xa = (((size_t)i * (p.rows_x / 256) + x / 2) * nq) * 4096 + (size_t)(x % 2) * 2048;
-                const size_t yb = (((size_t)j * (p.rows_y / 256) + y) * nq) * 4096;
-                const uint16_t* ah = p.Xhi + xa;
-                const uint16_t* al = p.Xlo + xa;
-                const uint16_t* bh = p.Yhi + yb;
-                const uint16_t* bl = p.Ylo + yb;
-                for (int kq = 0; kq < nk; kq += KS) {
-                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
+        // producer: lane 0 issues the copies, the whole warp paces
+        WavePacer pacer;
+        pacer.init(p.pace, (int)gridDim.x, p.pace_every, p.pace_slack);
+        uint32_t stage = 0, phase = 0, fill_phase = 0, filled = 0;
+        bool stop = false;
+        for (long long u = first; u < units && !stop; u += step) {
+            const long long pr = u / per_pair, bb = u % per_pair;
+            int ii, jj;
+            vtile_pair(p, pr, ii, jj);
+            const int i = p.i0 + ii, j = p.j0 + jj;
+            const int x = (int)(bb / p.nby), y = (int)(bb % p.nby);
+            // slab bases at Q step 0 (256-row blocks of nqc steps, 4096 elements a step)
+            const size_t nq = (size_t)p.nqc;
+            const size_t xa = (((size_t)i * (p.rows_x / 256) + x / 2) * nq) * 4096 + (size_t)(x % 2) * 2048;
+            const size_t yb = (((size_t)j * (p.rows_y / 256) + y) * nq) * 4096;
+            const uint16_t* ah = p.Xhi + xa;
+            const uint16_t* al = p.Xlo + xa;
+            const uint16_t* bh = p.Yhi + yb;
+            const uint16_t* bl = p.Ylo + yb;
+            for (int kq = 0; kq < nk; kq += KS) {
+                pacer.step(lane, kPaceLimitNs);
+                int ok = 1;
+                if (lane == 0) {
+                    if (*abort_flag) {
+                        ok = 0;
+                    } else if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
                         atomicExch(p.err, 21);
                         *abort_flag = 1;
-                        break;
+                        ok = 0;
+                    } else {
+                        const int nks = min(KS, nk - kq);
+                        uint8_t* sb = smem + stage * STAGE_BYTES;
+                        mbar_arrive_expect_tx(&full[stage], (uint32_t)nks * 2 * (SLAB_A + SLAB_B));
+                        const size_t kk = (size_t)kq * 4096;
+                        for (int q2 = 0; q2 < nks; ++q2) {
+                            bulk_g2s(sb + OFF_AH + q2 * SLAB_A, ah + kk + q2 * 4096, SLAB_A, &full[stage]);
+                            bulk_g2s(sb + OFF_AL + q2 * SLAB_A, al + kk + q2 * 4096, SLAB_A, &full[stage]);
+                        }
+                        bulk_g2s(sb + OFF_BH, bh + kk, nks * SLAB_B, &full[stage]);
+                        bulk_g2s(sb + OFF_BL, bl + kk, nks * SLAB_B, &full[stage]);
                     }
-                    const int nks = min(KS, nk - kq);
-                    uint8_t* sb = smem + stage * STAGE_BYTES;
-                    mbar_arrive_expect_tx(&full[stage], (uint32_t)nks * 2 * (SLAB_A + SLAB_B));
-                    const size_t kk = (size_t)kq * 4096;
-                    for (int q2 = 0; q2 < nks; ++q2) {
-                        bulk_g2s(sb + OFF_AH + q2 * SLAB_A, ah + kk + q2 * 4096, SLAB_A, &full[stage]);
-                        bulk_g2s(sb + OFF_AL + q2 * SLAB_A, al + kk + q2 * 4096, SLAB_A, &full[stage]);
-                    }
-                    bulk_g2s(sb + OFF_BH, bh + kk, nks * SLAB_B, &full[stage]);
-                    bulk_g2s(sb + OFF_BL, bl + kk, nks * SLAB_B, &full[stage]);
-                    fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
-                    filled |= 1u << stage;
-                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    stop = true;
+                    break;
+                }
+                fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
+                filled |= 1u << stage;
+                if (++stage == STAGES) { stage = 0; phase ^= 1; }
             }
+        }
+        pacer.finish(lane);
+        if (lane == 0) {
             if (!*abort_flag) {
                 for (int s = 0; s < STAGES; ++s) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {

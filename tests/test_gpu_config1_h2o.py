@@ -55,8 +55,15 @@ def test_config1_integral_direct_decomposition():
     """The integral-direct decomposition (mshqc_cd_cholesky_direct: ERI
     diagonal and columns from the host engine, the vectors on the GPU, the
     reference's DirectCholesky of src/integrals/cholesky_direct.cc) against the
-    decomposition of the full ERI tensor: the same pivots, hence the same
-    vectors to rounding, and the same CD-RMP2 energy to 1e-10 Eh."""
+    decomposition of the full ERI tensor.  The two need not pick the same
+    pivots: H2O's diagonal is full of ties ((mn|mn) = (nm|nm) always, and the
+    two H atoms are equivalent; 166 of the 182 steps choose among near-equal
+    maxima), so the first argmax depends on the last bit of each diagonal
+    update and the vectors may come out in another order or basis.  What they
+    represent must agree: the same number of vectors, each set reproducing
+    the ERI matrix within the stopping threshold (the residual is positive
+    semidefinite, so its largest entry is its largest diagonal element), and
+    the same CD-RMP2 energy to 1e-10 Eh."""
     fix = json.load(open(os.path.join(HERE, "golden", "h2o_basis_sets.json")))
     case = fix["cases"]["mshqc_h2o_ccpvdz"]
     mol = ao.Molecule.from_angstrom(case["atoms"], case["angstrom_to_bohr"])
@@ -75,8 +82,11 @@ def test_config1_integral_direct_decomposition():
         Ld = ctx.cholesky_direct(bs, 1e-6)
         ctx.set_orbitals(capi.ALPHA, C, e, 5)
         ed = ctx.mp2_energy(capi.RESTRICTED, capi.FP64)["total"]
-    print(f"\nintegral-direct: {Ld.shape[0]} vectors (full tensor: {Lf.shape[0]}), max |dL| "
-          f"{np.max(np.abs(Ld - Lf)):.2e}, energy difference {abs(ed - ef):.2e} Eh")
+    G = g.reshape(Lf.shape[1], Lf.shape[1])
+    res_d = np.max(np.abs(G - Ld.T @ Ld))
+    res_f = np.max(np.abs(G - Lf.T @ Lf))
+    print(f"\nintegral-direct: {Ld.shape[0]} vectors (full tensor: {Lf.shape[0]}), max |G - L^T L| "
+          f"{res_d:.2e} ({res_f:.2e}), energy difference {abs(ed - ef):.2e} Eh")
     assert Ld.shape == Lf.shape
-    assert np.max(np.abs(Ld - Lf)) <= 1e-10
+    assert res_d <= 1e-6 and res_f <= 1e-6
     assert abs(ed - ef) <= 1e-10
