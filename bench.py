@@ -451,6 +451,7 @@ def bench_gpu(args, w, rank, world, local_rank):
     for _ in range(args.steps):
         r = step(ctx, prec, C_dev, e_dev)
         stages.append(ctx.stage_times())
+    stage_n = ctx.stage_counts()
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -581,7 +582,7 @@ def bench_gpu(args, w, rank, world, local_rank):
         peak = peaks["bf16_tflops_sustained"] / 3.0
         peak_note = (f"dense 16-bit tensor peak ({peak_src}, sustained "
                      f"{peaks['bf16_tflops_sustained']}) / 3: three products per useful product")
-    traffic = roofline_traffic(kname, w)
+    traffic = roofline_traffic(kname, w, stage_n.get(dom, 0), world if shared else 1)
 
     if rank == 0:
         line = {
@@ -610,8 +611,10 @@ def bench_gpu(args, w, rank, world, local_rank):
             "roofline": {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic.get("bytes") if traffic else None,
+                         "algorithmic_bytes": traffic.get("algorithmic_bytes") if traffic else None,
                          "traffic_note": traffic.get("note") if traffic else "no capture for this kernel",
-                         "peak_source": peak_note, "kernel_ms_per_step": kms},
+                         "peak_source": peak_note, "kernel_ms_per_step": kms,
+                         "kernel_launches_per_step": stage_n.get(dom, 0)},
         }
         if not args.no_cpu_baseline:
             try:
@@ -621,11 +624,47 @@ def bench_gpu(args, w, rank, world, local_rank):
         print(json.dumps(line))
 
 
-def roofline_traffic(kname, w):
-    """DRAM bytes per launch of the dominant kernel from the ncu captures
-    summarised under profiles/ (one small launch captured, scaled to this
-    workload's launch by the tiles it processes); None without a capture."""
-    return None
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one captured
+# launch of the dominant kernel, with the extent of that launch: the Gamma
+# GEMM of the first block pair of the default step (R = K = 30 occupied
+# orbitals x 1920 padded virtuals, Q = 8192, 30 x 1800 rows of Gamma
+# read-modified-written), captured in one ncu pass with wave pacing and
+# 16-row-block tile groups (profiles/gamma_tc_kernel_cdmp2_grad_n2000_o200_m8000.md).
+# A wave of Gamma tiles reads its operand rows once per K step and a launch
+# has R / 128 * Q / 256 / 148 waves, so the operand traffic of a launch grows
+# as R * K; the read-modify-write of Gamma adds 16 bytes per written element.
+CAPTURED_TRAFFIC = {
+    "gamma_tc_kernel": {"bytes": 83754782976 + 2930398976, "R": 57600, "K": 57600,
+                        "rmw": 16 * 30 * 1800 * 8000},
+}
+
+
+def roofline_traffic(kname, w, launches, share):
+    """DRAM bytes per launch of the dominant kernel: the captured launch
+    (CAPTURED_TRAFFIC) scaled to this step by the operand extent its
+    launches process, averaged over them; None where there is no capture.
+    The restricted backward over nb occupied blocks makes nb^2 Gamma
+    launches (nb diagonal, two per off-diagonal block pair) whose R * K add
+    up to (o * VR)^2 and whose Gamma rows add up to nb * o * v; a rank of a
+    shared gradient makes about nb^2 / share of them."""
+    cap = CAPTURED_TRAFFIC.get(kname)
+    if cap is None or not w.get("gradient") or w.get("kind") == "unrestricted" or launches <= 0:
+        return None
+    N, o, M = w["N"], w["o"], w["M"]
+    v = N - o
+    VR = 128 * ((v + 127) // 128)
+    nb = max(1, round((launches * share) ** 0.5))
+    per_rk = (cap["bytes"] - cap["rmw"]) / (cap["R"] * cap["K"])
+    step_bytes = per_rk * float(o * VR) ** 2 + 16.0 * v * M * o * nb
+    per_launch = step_bytes / (nb * nb)
+    # algorithmic: amplitudes (BF16 hi/lo) and B^T (hi/lo) once, Gamma rows once
+    Q = 256 * ((M + 255) // 256)
+    algo = (4.0 * float(o * VR) ** 2 + 4.0 * Q * nb * o * VR + 16.0 * v * M * o * nb) / (nb * nb)
+    return {"bytes": per_launch, "algorithmic_bytes": algo,
+            "note": (f"ncu capture of one launch (R=K={cap['R']}: {cap['bytes'] / 1e9:.1f} GB) scaled by "
+                     f"the operand extent to this step's {nb * nb} launches "
+                     f"({step_bytes / 1e12:.2f} TB per step, {per_launch / 1e9:.1f} GB per launch; "
+                     f"algorithmic {algo / 1e9:.1f} GB per launch)")}
 
 
 def main():

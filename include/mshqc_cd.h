@@ -155,6 +155,11 @@ MSHQC_CD_API int mshqc_cd_launch_count(mshqc_cd_ctx* ctx, int64_t* count);
  * transforms, [6] other, [7] element-wise amplitude pass.  n_out entries are
  * written (at most 8). */
 MSHQC_CD_API int mshqc_cd_stage_times(mshqc_cd_ctx* ctx, double* ms_out, int n_out);
+/* Timed intervals per stage of the last call, in the order of
+ * mshqc_cd_stage_times.  In the mixed-precision backward each integral-tile
+ * and each Gamma interval is one kernel launch, so stage_times / stage_counts
+ * is the average launch duration of those kernels. */
+MSHQC_CD_API int mshqc_cd_stage_counts(mshqc_cd_ctx* ctx, int64_t* n_out, int n);
 /* 1 when every tensor-core accumulation of the last mixed-precision call was
  * provably exact (Cauchy-Schwarz bound of the integer accumulators below
  * 2^24 and no accumulator seen at 2^24), else 0. */

@@ -78,6 +78,7 @@ SIGNATURES = {
     "mshqc_cd_device_bytes": (_i32, [_vp, ctypes.POINTER(_i64)]),
     "mshqc_cd_launch_count": (_i32, [_vp, ctypes.POINTER(_i64)]),
     "mshqc_cd_stage_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
+    "mshqc_cd_stage_counts": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), _i32]),
     "mshqc_cd_mixed_exact": (_i32, [_vp, ctypes.POINTER(_i32)]),
     "mshqc_cd_set_vectors": (_i32, [_vp, _vp, _i64, _i64, _i32, _i32]),
     "mshqc_cd_set_orbitals": (_i32, [_vp, _i32, _vp, _vp, _i64, _i32]),
@@ -240,6 +241,13 @@ class Context:
         buf = (ctypes.c_double * 8)()
         _check(self._lib.mshqc_cd_stage_times(self._h, buf, 8))
         return {name: buf[k] for k, name in enumerate(self.STAGES)}
+
+    def stage_counts(self) -> dict:
+        """Timed intervals per stage of the last call (one per launch of the
+        integral-tile and Gamma kernels of the mixed-precision backward)."""
+        buf = (ctypes.c_int64 * 8)()
+        _check(self._lib.mshqc_cd_stage_counts(self._h, buf, 8))
+        return {name: int(buf[k]) for k, name in enumerate(self.STAGES)}
 
     def mixed_exact(self) -> bool:
         x = ctypes.c_int(0)

@@ -34,6 +34,7 @@ thread_local std::string g_last_error = "";
 namespace mshqc_cd {
 void reset_stages(mshqc_cd_ctx* ctx) {
     for (double& t : ctx->stage_ms) t = 0.0;
+    for (int64_t& n : ctx->stage_n) n = 0;
     ctx->ev_marks.clear();
     ctx->ev_used = 0;
 }
@@ -60,8 +61,10 @@ void collect_stages(mshqc_cd_ctx* ctx) {
     for (const auto& m : ctx->ev_marks) {
         if ((size_t)m.second + 1 >= ctx->ev_used) continue;
         float ms = 0.0f;
-        if (cudaEventElapsedTime(&ms, ctx->ev_pool[m.second], ctx->ev_pool[m.second + 1]) == cudaSuccess)
+        if (cudaEventElapsedTime(&ms, ctx->ev_pool[m.second], ctx->ev_pool[m.second + 1]) == cudaSuccess) {
             ctx->stage_ms[m.first] += ms;
+            ctx->stage_n[m.first] += 1;
+        }
     }
     ctx->ev_marks.clear();
     ctx->ev_used = 0;
@@ -327,6 +330,13 @@ int mshqc_cd_stage_times(mshqc_cd_ctx* ctx, double* ms_out, int n_out) {
     CD_CHECK_CTX();
     if (!ms_out || n_out < 0) return set_error(MSHQC_CD_ERR_ARG, "bad output");
     for (int k = 0; k < n_out && k < 8; ++k) ms_out[k] = ctx->stage_ms[k];
+    return MSHQC_CD_OK;
+}
+
+int mshqc_cd_stage_counts(mshqc_cd_ctx* ctx, int64_t* n_out, int n) {
+    CD_CHECK_CTX();
+    if (!n_out || n < 0) return set_error(MSHQC_CD_ERR_ARG, "bad output");
+    for (int k = 0; k < n && k < 8; ++k) n_out[k] = ctx->stage_n[k];
     return MSHQC_CD_OK;
 }
 

@@ -67,6 +67,7 @@ struct mshqc_cd_ctx {
     int64_t launches = 0;           // kernels launched by this context
     // per-stage device timing of the last call (see mshqc_cd_stage_times)
     double stage_ms[8] = {};
+    int64_t stage_n[8] = {};        // timed intervals per stage of the last call
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, int>> ev_marks;   // (stage, index of the start event)
     size_t ev_used = 0;

@@ -65,7 +65,7 @@ constexpr size_t kPartF64Budget = size_t(8) << 30;
 // copies per epoch and epochs of slack; MSHQC_CD_PACE=off disables it,
 // MSHQC_CD_PACE=<every>,<slack> sets both.
 void pace_params(int* every, int* slack) {
-    *every = 8;
+    *every = 16;
     *slack = 2;
     const char* env = std::getenv("MSHQC_CD_PACE");
     if (!env) return;
