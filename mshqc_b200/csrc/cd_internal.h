@@ -38,13 +38,14 @@ struct SpinState {
     bool B64_valid = false;
     int B64_prec = 0;       // MSHQC_CD_FP64: FP64 products; MSHQC_CD_FP16X3: int8-slice products
     // fixed-point hi/lo (BF16 carriers) of the MO vectors for the tensor-core path
-    DevBuf Bhi, Blo;
+    DevBuf Bhi, Blo;        // Blo unused in the pair layout (hi and lo interleaved in Bhi)
     DevBuf expo;            // per-row power-of-two exponents [o][rows]
     DevBuf diag;            // exact (ia|ia) [o][rows]
     DevBuf norms;           // sum hi^2, sum lo^2 per row [2][o][rows]
     int64_t vp16 = 0, Mp16 = 0;
     double max_norm_hi = 0, max_norm_lo = 0;
     bool B16_valid = false;
+    int B16_layout = 0;     // 0: integral-tile layout, 1: pair layout (split_bf16.cuh)
     void invalidate() {
         B64_valid = false;
         B16_valid = false;
@@ -232,7 +233,9 @@ int check_finite_device(mshqc_cd_ctx* ctx, const double* x, int64_t n, const cha
     } while (0)
 
 // implemented in cd_mp2.cu
-int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision);
+// layout: of the fixed-point operands of a mixed-precision request
+// (0: integral tiles of the backward, 1: fused pair energies)
+int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision, int layout = 0);
 int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out);
 int run_gradient(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* e_out,
                  double* dC_a, double* dC_b, double* deps_a, double* deps_b, int where);

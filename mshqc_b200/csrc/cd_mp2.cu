@@ -62,12 +62,13 @@ constexpr size_t kPartTcBudget = size_t(16) << 30;
 constexpr size_t kPartF64Budget = size_t(8) << 30;
 
 // Wave pacing of the persistent tile kernels (WavePacer in sm100_ptx.cuh):
-// copies per epoch and epochs of slack; MSHQC_CD_PACE=off disables it,
-// MSHQC_CD_PACE=<every>,<slack> sets both.
-void pace_params(int* every, int* slack) {
+// copies per epoch and epochs of slack.  MSHQC_CD_PACE (Gamma) and
+// MSHQC_CD_PACE_TILES (integral tiles) = off disables it, = <every>,<slack>
+// sets both.
+void pace_params(int* every, int* slack, const char* var = "MSHQC_CD_PACE") {
     *every = 16;
     *slack = 2;
-    const char* env = std::getenv("MSHQC_CD_PACE");
+    const char* env = std::getenv(var);
     if (!env) return;
     if (std::strcmp(env, "off") == 0) {
         *every = 0;
@@ -437,13 +438,14 @@ int64_t tc_rows(int64_t v) { return 128 * round_up(cdiv(v, 128), 2); }
 
 // fixed-point hi/lo split of one spin's FP64 MO vectors into the blocked layout,
 // with the per-row exponents, exact diagonal integrals and hi/lo row norms
-int split_fixed(mshqc_cd_ctx* ctx, int spin) {
+int split_fixed(mshqc_cd_ctx* ctx, int spin, int layout) {
     SpinState& s = ctx->spin[spin];
     const int64_t o = s.nocc, v = ctx->N - s.nocc, M = ctx->M, Mp = ctx->Mp;
     const int64_t rows = tc_rows(v), nqc = Mp / 16;
     const size_t n = (size_t)o * nqc * rows * 16;
-    CD_ALLOC(s.Bhi, n * sizeof(uint16_t), false);
-    CD_ALLOC(s.Blo, n * sizeof(uint16_t), false);
+    const bool pair_layout = layout == 1;
+    CD_ALLOC(s.Bhi, (pair_layout ? 2 : 1) * n * sizeof(uint16_t), false);
+    if (!pair_layout) CD_ALLOC(s.Blo, n * sizeof(uint16_t), false);
     CD_ALLOC(s.expo, sizeof(int) * o * rows, true);
     CD_ALLOC(s.diag, sizeof(double) * o * rows, true);
     CD_ALLOC(s.norms, sizeof(double) * 2 * o * rows, true);
@@ -465,7 +467,7 @@ int split_fixed(mshqc_cd_ctx* ctx, int spin) {
         const int blocks = (int)std::min<int64_t>(cdiv(threads, 256), (int64_t)ctx->num_sms * 16);
         split_fixed_blocked_kernel<<<blocks, 256, 0, ctx->stream>>>(
             s.B64.as<double>(), s.vp, Mp, (int)v, (int)M, o, nqc, rows, s.expo.as<int>(),
-            s.Bhi.as<uint16_t>(), s.Blo.as<uint16_t>());
+            s.Bhi.as<uint16_t>(), pair_layout ? nullptr : s.Blo.as<uint16_t>(), pair_layout);
         CD_CUDA(cudaGetLastError());
         ctx->launches++;
     }
@@ -480,6 +482,7 @@ int split_fixed(mshqc_cd_ctx* ctx, int spin) {
         s.max_norm_lo = std::max(s.max_norm_lo, hn[o * rows + r]);
     }
     s.B16_valid = true;
+    s.B16_layout = layout;
     return MSHQC_CD_OK;
 }
 
@@ -575,9 +578,11 @@ int pair_pass_tc(mshqc_cd_ctx* ctx, int mode, int sx, int sy, double* total,
         CD_RC(opposite_spin_diag(ctx));
         end_stage(ctx);
     }
+    if (X.B16_layout != 1 || Y.B16_layout != 1)
+        return set_error(MSHQC_CD_ERR_STATE, "fixed-point operands not in the pair layout");
     PairTcArgs a{};
-    a.Xhi = X.Bhi.as<uint16_t>();  a.Xlo = X.Blo.as<uint16_t>();
-    a.Yhi = Y.Bhi.as<uint16_t>();  a.Ylo = Y.Blo.as<uint16_t>();
+    a.Xp = X.Bhi.as<uint16_t>();
+    a.Yp = Y.Bhi.as<uint16_t>();
     a.ex = X.expo.as<int>();  a.ey = Y.expo.as<int>();
     if (mode == PAIR_OPPOSITE_SPIN) {
         a.diag = ctx->diag_os.as<double>();
@@ -628,7 +633,7 @@ int invalidate_spin(mshqc_cd_ctx* ctx, int spin) {
     return MSHQC_CD_OK;
 }
 
-int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
+int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision, int layout) {
     CD_RC(require_inputs(ctx, spin));
     SpinState& s = ctx->spin[spin];
     if (precision != MSHQC_CD_FP64 && precision != MSHQC_CD_FP16X3)
@@ -648,9 +653,9 @@ int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision) {
         end_stage(ctx);
         s.B16_valid = false;
     }
-    if (precision == MSHQC_CD_FP16X3 && !s.B16_valid) {
+    if (precision == MSHQC_CD_FP16X3 && (!s.B16_valid || s.B16_layout != layout)) {
         begin_stage(ctx, ST_SPLIT);
-        CD_RC(split_fixed(ctx, spin));
+        CD_RC(split_fixed(ctx, spin, layout));
         end_stage(ctx);
     }
     return MSHQC_CD_OK;
@@ -669,8 +674,8 @@ int run_energy(mshqc_cd_ctx* ctx, int kind, int precision, mshqc_cd_energy* out)
     if (kind == MSHQC_CD_UNRESTRICTED) CD_RC(require_inputs(ctx, 1));
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     CD_CUDA(cudaEventRecord(e0, ctx->stream));
-    CD_RC(ensure_transform(ctx, 0, precision));
-    if (kind == MSHQC_CD_UNRESTRICTED) CD_RC(ensure_transform(ctx, 1, precision));
+    CD_RC(ensure_transform(ctx, 0, precision, 1));
+    if (kind == MSHQC_CD_UNRESTRICTED) CD_RC(ensure_transform(ctx, 1, precision, 1));
     CD_CUDA(cudaEventRecord(e1, ctx->stream));
     for (auto& p : ctx->pair_energy) p.clear();
     if (kind == MSHQC_CD_RESTRICTED) {
@@ -1089,6 +1094,8 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
     double* prow = ctx->dsum.as<double>();
     double* pcol = prow + npairs * dx.VR;
     double* pocc = pcol + npairs * dy.VR;
+    if (X.B16_layout != 0 || Y.B16_layout != 0)
+        return set_error(MSHQC_CD_ERR_STATE, "fixed-point operands not in the integral-tile layout");
     const size_t vsm = vtile_tc::SMEM_BYTES;
     CD_CUDA(cudaFuncSetAttribute(vtile_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
     for (int64_t I0 = 0; I0 < dx.o; I0 += bI) {
@@ -1117,7 +1124,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             a.tri = tri ? 1 : 0;
             const int64_t vunits = (int64_t)npl * a.nbx * a.nby;
             const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
-            pace_params(&a.pace_every, &a.pace_slack);
+            pace_params(&a.pace_every, &a.pace_slack, "MSHQC_CD_PACE_TILES");
             if (a.pace_every > 0) {
                 CD_ALLOC(ctx->pace, sizeof(int) * (size_t)vgrid, true);
                 a.pace = ctx->pace.as<int>();

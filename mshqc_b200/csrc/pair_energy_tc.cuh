@@ -1,24 +1,25 @@
 // Fused pair-energy kernel on the 5th-generation tensor cores (tcgen05), exact
 // fixed-point accumulation (split_bf16.cuh describes the hi/lo encoding).
 //
-// Operands live in a "core-matrix blocked" layout so that every operand slab
-// is one contiguous run of bytes that lands in shared memory already in the
-// canonical K-major no-swizzle UMMA layout (split_bf16.cuh):
-//
-//   element (i, a, Q) at  ((i*rows/256 + a/256)*nqc + Q/16)*4096
-//                         + ((a%256)/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
-//
-// A slab = rows [a0, a0+128) x one 16-wide Q chunk = 4 KB contiguous; the
-// slabs of consecutive chunks are 8 KB apart.
+// Operands are the fixed-point hi/lo of split_bf16.cuh in its pair layout:
+// 128-row blocks whose 16-wide Q chunks hold the hi slab (4 KB) and then the
+// lo slab (4 KB) of the same rows, chunks one after the other, each slab in
+// the canonical K-major no-swizzle UMMA layout.  So one contiguous copy
+// brings both halves of an operand for KS = 2 chunks (16 KB), and a chunk's
+// [hi; lo] is one 256-row operand.
 //
 // Work unit = pair (i,j), row block x (128 virtuals a), column block y (128
-// virtuals b).  Per Q chunk the MMA thread issues six 128x128x16 MMAs into
-// four TMEM accumulators (columns):
-//   [  0,128) T1hh = Xhi_i[x] . Yhi_j[y]
-//   [128,256) T1x  = Xhi_i[x] . Ylo_j[y] + Xlo_i[x] . Yhi_j[y]
-//   [256,384) T2hh, [384,512) T2x   the same for slabs P2, P3
-// RESTRICTED / SAME_SPIN: P2 = X_j[x], P3 = X_i[y]  ->  T2 = (ib|ja) at (a,b);
-// OPPOSITE_SPIN: P2 = P0, P3 = Y_j[y+1]            ->  T2 = (ia|jb') of the next block.
+// virtuals b).  Per Q chunk the MMA thread issues four MMAs into four TMEM
+// accumulators (columns):
+//   [  0,256) P0hi . [P1hi; P1lo]  (N = 256): T1hh in [0,128), hi*lo' in [128,256)
+//   [128,256) += P0lo . P1hi       (N = 128): T1x = hi*lo' + lo*hi'
+//   [256,512) the same for P2, P3: T2hh in [256,384), T2x in [384,512)
+// RESTRICTED / SAME_SPIN: P0 = X_i[x], P1 = X_j[y], P2 = X_j[x], P3 = X_i[y]
+//   ->  T1 = (ia|jb), T2 = (ib|ja) at (a,b);
+// OPPOSITE_SPIN: P2 = P0, P3 = Y_j[y+1]  ->  T2 = (ia|jb') of the next block.
+// A stage holds the four operands' copies for two chunks (64 KB), three
+// stages.  The previous form (one 4 KB copy per slab and chunk, six N=128
+// MMAs) was bound by the copy rate: eight copies per chunk.
 // All accumulator entries are exact integers, so the epilogue recovers
 //   (ia|jb) = u_ia u_jb (T1hh + T1x / 256)
 // exactly in FP64, substitutes the exact FP64 (ia|ia) on the diagonal, forms
@@ -42,8 +43,8 @@
 namespace mshqc_cd {
 
 struct PairTcArgs {
-    const uint16_t* Xhi; const uint16_t* Xlo;   // blocked FP16 bits, spin X
-    const uint16_t* Yhi; const uint16_t* Ylo;   // spin Y (== X for RESTRICTED / SAME_SPIN)
+    const uint16_t* Xp;     // fixed-point FP16 bits of spin X, pair layout (split_bf16.cuh)
+    const uint16_t* Yp;     // spin Y (== X for RESTRICTED / SAME_SPIN)
     const int* ex; const int* ey;               // row exponents [o][rows]
     const double* diag;                         // exact (ia|ia): [ox][rows_x] (RESTRICTED)
                                                 // or sum_Q Xa*Yb [diag_o][rows_x] (OPPOSITE)
@@ -66,12 +67,13 @@ namespace pair_tc {
 constexpr int BM = 128;
 constexpr int BN = 128;
 constexpr int KC = 16;
-constexpr int STAGES = 6;
+constexpr int KS = 2;                      // Q chunks per stage
+constexpr int STAGES = 3;
 constexpr int THREADS = 192;
-constexpr uint32_t SLAB = 128 * KC * 2;    // 4096 bytes
-// stage layout: P0hi P1hi P2hi P3hi P0lo P1lo P2lo P3lo
-constexpr uint32_t HALF = 4 * SLAB;                          // 16384
-constexpr uint32_t STAGE_BYTES = 2 * HALF;                   // 32768
+constexpr uint32_t SLAB = 128 * KC * 2;    // 4096 bytes: 128 rows x one chunk, hi or lo
+constexpr uint32_t CHUNK = 2 * SLAB;       // hi and lo of one chunk
+constexpr uint32_t PIECE = KS * CHUNK;     // one operand of a stage (16 KB)
+constexpr uint32_t STAGE_BYTES = 4 * PIECE;                  // 65536: P0 P1 P2 P3
 constexpr uint32_t SMEM_DATA = STAGES * STAGE_BYTES;         // 196608
 // after the data: barriers (< 256 B), reduction scratch (64 B at +256),
 // per-unit column tables at +512: eps (2 x 128 doubles), column scales
@@ -139,44 +141,37 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                 const int2 ij = p.pairs[u / p.nblocks];
                 const int2 xy = p.blocks[u % p.nblocks];
                 const size_t a0 = (size_t)xy.x * BM, b0 = (size_t)xy.y * BN;
-                // slab bases at Q chunk 0 (element offset of the 128 rows from r0
-                // of orbital o); chunk kq adds kq * 4096 elements
-                const size_t nbx = (size_t)p.rows_x / 256, nby = (size_t)p.rows_y / 256, nq = (size_t)p.nqc;
-                auto slab_x = [&](size_t o, size_t r0) { return ((o * nbx + r0 / 256) * nq) * 4096 + (r0 % 256) * 16; };
-                auto slab_y = [&](size_t o, size_t r0) { return ((o * nby + r0 / 256) * nq) * 4096 + (r0 % 256) * 16; };
-                const uint16_t *s0h, *s1h, *s2h, *s3h, *s0l, *s1l, *s2l, *s3l;
-                const size_t c0 = 4096, c1 = 4096, c2 = 4096, c3 = 4096;
+                // operand bases at Q chunk 0 (the 128 rows from r0 of orbital
+                // o); chunk kq adds kq * 4096 elements (hi and lo)
+                const size_t nbx = (size_t)p.rows_x / 128, nby = (size_t)p.rows_y / 128, nq = (size_t)p.nqc;
+                auto slab_x = [&](size_t o, size_t r0) { return ((o * nbx + r0 / 128) * nq) * 4096; };
+                auto slab_y = [&](size_t o, size_t r0) { return ((o * nby + r0 / 128) * nq) * 4096; };
+                const uint16_t *s0, *s1, *s2, *s3;
                 if (MODE == PAIR_OPPOSITE_SPIN) {
-                    s0h = p.Xhi + slab_x(ij.x, a0);       s0l = p.Xlo + slab_x(ij.x, a0);
-                    s1h = p.Yhi + slab_y(ij.y, b0);       s1l = p.Ylo + slab_y(ij.y, b0);
-                    s2h = s0h;                            s2l = s0l;
-                    s3h = p.Yhi + slab_y(ij.y, b0 + BN);  s3l = p.Ylo + slab_y(ij.y, b0 + BN);
+                    s0 = p.Xp + slab_x(ij.x, a0);
+                    s1 = p.Yp + slab_y(ij.y, b0);
+                    s2 = s0;
+                    s3 = p.Yp + slab_y(ij.y, b0 + BN);
                 } else {
-                    s0h = p.Xhi + slab_x(ij.x, a0);  s0l = p.Xlo + slab_x(ij.x, a0);
-                    s1h = p.Xhi + slab_x(ij.y, b0);  s1l = p.Xlo + slab_x(ij.y, b0);
-                    s2h = p.Xhi + slab_x(ij.y, a0);  s2l = p.Xlo + slab_x(ij.y, a0);
-                    s3h = p.Xhi + slab_x(ij.x, b0);  s3l = p.Xlo + slab_x(ij.x, b0);
+                    s0 = p.Xp + slab_x(ij.x, a0);
+                    s1 = p.Xp + slab_x(ij.y, b0);
+                    s2 = p.Xp + slab_x(ij.y, a0);
+                    s3 = p.Xp + slab_x(ij.x, b0);
                 }
-                const uint32_t bytes = (MODE == PAIR_OPPOSITE_SPIN) ? 6 * SLAB : 8 * SLAB;
-                for (int kq = 0; kq < nk; ++kq) {
+                for (int kq = 0; kq < nk; kq += KS) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1, kWaitLimitNs)) {
                         atomicExch(p.err, 1);
                         *abort_flag = 1;
                         break;
                     }
+                    const uint32_t bytes = (uint32_t)min(KS, nk - kq) * CHUNK;
                     uint8_t* sb = smem + stage * STAGE_BYTES;
-                    mbar_arrive_expect_tx(&full[stage], bytes);
-                    const size_t k = (size_t)kq;
-                    bulk_g2s(sb + 0 * SLAB, s0h + k * c0, SLAB, &full[stage]);
-                    bulk_g2s(sb + HALF + 0 * SLAB, s0l + k * c0, SLAB, &full[stage]);
-                    bulk_g2s(sb + 1 * SLAB, s1h + k * c1, SLAB, &full[stage]);
-                    bulk_g2s(sb + HALF + 1 * SLAB, s1l + k * c1, SLAB, &full[stage]);
-                    if (MODE != PAIR_OPPOSITE_SPIN) {
-                        bulk_g2s(sb + 2 * SLAB, s2h + k * c2, SLAB, &full[stage]);
-                        bulk_g2s(sb + HALF + 2 * SLAB, s2l + k * c2, SLAB, &full[stage]);
-                    }
-                    bulk_g2s(sb + 3 * SLAB, s3h + k * c3, SLAB, &full[stage]);
-                    bulk_g2s(sb + HALF + 3 * SLAB, s3l + k * c3, SLAB, &full[stage]);
+                    mbar_arrive_expect_tx(&full[stage], (MODE == PAIR_OPPOSITE_SPIN ? 3u : 4u) * bytes);
+                    const size_t k = (size_t)kq * 4096;
+                    bulk_g2s(sb + 0 * PIECE, s0 + k, bytes, &full[stage]);
+                    bulk_g2s(sb + 1 * PIECE, s1 + k, bytes, &full[stage]);
+                    if (MODE != PAIR_OPPOSITE_SPIN) bulk_g2s(sb + 2 * PIECE, s2 + k, bytes, &full[stage]);
+                    bulk_g2s(sb + 3 * PIECE, s3 + k, bytes, &full[stage]);
                     fill_phase = (fill_phase & ~(1u << stage)) | (phase << stage);
                     filled |= 1u << stage;
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
@@ -201,7 +196,8 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
-            constexpr uint32_t IDESC = idesc_f16_f32(BM, BN);
+            constexpr uint32_t IDESC = idesc_f16_f32(BM, BN);          // N = 128
+            constexpr uint32_t IDESC2 = idesc_f16_f32(BM, 2 * BN);     // N = 256: [hi; lo]
             uint32_t stage = 0, phase = 0, acc_phase = 0;
             const uint32_t sbase = smem_addr(smem);
             for (long long u = first; u < p.units && !*abort_flag; u += step) {
@@ -213,7 +209,7 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                 }
                 acc_phase ^= 1;
                 tc_fence_after();
-                for (int kq = 0; kq < nk; ++kq) {
+                for (int kq = 0; kq < nk; kq += KS) {
                     if (!mbar_wait_bounded(&full[stage], phase, kWaitLimitNs)) {
                         atomicExch(p.err, 3);
                         *abort_flag = 1;
@@ -221,21 +217,21 @@ __global__ void __launch_bounds__(192, 1) pair_energy_tc_kernel(PairTcArgs p) {
                     }
                     tc_fence_after();
                     const uint32_t sb = sbase + stage * STAGE_BYTES;
-                    const uint64_t p0h = smem_desc_kmajor(sb + 0 * SLAB, 128, 256);
-                    const uint64_t p1h = smem_desc_kmajor(sb + 1 * SLAB, 128, 256);
-                    const uint64_t p3h = smem_desc_kmajor(sb + 3 * SLAB, 128, 256);
-                    const uint64_t p0l = smem_desc_kmajor(sb + HALF + 0 * SLAB, 128, 256);
-                    const uint64_t p1l = smem_desc_kmajor(sb + HALF + 1 * SLAB, 128, 256);
-                    const uint64_t p3l = smem_desc_kmajor(sb + HALF + 3 * SLAB, 128, 256);
-                    const uint64_t p2h = (MODE == PAIR_OPPOSITE_SPIN) ? p0h : smem_desc_kmajor(sb + 2 * SLAB, 128, 256);
-                    const uint64_t p2l = (MODE == PAIR_OPPOSITE_SPIN) ? p0l : smem_desc_kmajor(sb + HALF + 2 * SLAB, 128, 256);
-                    const uint32_t acc = kq > 0 ? 1u : 0u;
-                    mma_f16(tmem + 0, p0h, p1h, IDESC, acc);
-                    mma_f16(tmem + 128, p0h, p1l, IDESC, acc);
-                    mma_f16(tmem + 128, p0l, p1h, IDESC, 1u);
-                    mma_f16(tmem + 256, p2h, p3h, IDESC, acc);
-                    mma_f16(tmem + 384, p2h, p3l, IDESC, acc);
-                    mma_f16(tmem + 384, p2l, p3h, IDESC, 1u);
+                    const int nks = min(KS, nk - kq);
+                    for (int c = 0; c < nks; ++c) {
+                        const uint32_t o0 = sb + 0 * PIECE + c * CHUNK, o1 = sb + 1 * PIECE + c * CHUNK;
+                        const uint32_t o2 = (MODE == PAIR_OPPOSITE_SPIN ? sb : sb + 2 * PIECE) + c * CHUNK;
+                        const uint32_t o3 = sb + 3 * PIECE + c * CHUNK;
+                        // hi at +0, lo at +SLAB; [hi; lo] is the 256-row operand at +0
+                        const uint64_t p0h = smem_desc_kmajor(o0, 128, 256), p0l = smem_desc_kmajor(o0 + SLAB, 128, 256);
+                        const uint64_t p2h = smem_desc_kmajor(o2, 128, 256), p2l = smem_desc_kmajor(o2 + SLAB, 128, 256);
+                        const uint64_t p1 = smem_desc_kmajor(o1, 128, 256), p3 = smem_desc_kmajor(o3, 128, 256);
+                        const uint32_t acc = (kq + c) > 0 ? 1u : 0u;
+                        mma_f16(tmem + 0, p0h, p1, IDESC2, acc);     // hh | hi*lo'
+                        mma_f16(tmem + 128, p0l, p1, IDESC, 1u);     // + lo*hi'
+                        mma_f16(tmem + 256, p2h, p3, IDESC2, acc);
+                        mma_f16(tmem + 384, p2l, p3, IDESC, 1u);
+                    }
                     mma_commit(&empty[stage]);       // frees the stage when these MMAs finish
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }

@@ -99,16 +99,28 @@ static __global__ void row_scale_kernel(const double* __restrict__ src, int64_t 
 }
 
 // src: [o][vp][Mp] FP64 (zeros outside v x M); expo from row_scale_kernel.
-// dst: FP16 bits in 256-row blocks, each holding its nqc 16-wide Q chunks one
-// after the other, blocked inside a chunk as (a/8, (Q%16)/8, a%8, Q%8):
-//   element (i, a, Q) at ((i*rows/256 + a/256)*nqc + Q/16)*4096
-//                        + ((a%256)/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
-// (rows a multiple of 256), so a 128-row slab of one chunk is 4 KB and a
-// 256-row slab of consecutive chunks is one contiguous run.
+// dst, two layouts of FP16 bits, blocked inside a 16-wide Q chunk as
+// (a/8, (Q%16)/8, a%8, Q%8) (the canonical K-major no-swizzle UMMA layout):
+//  * pair_layout = false (integral tiles of the backward): hi and lo in
+//    separate arrays of 256-row blocks, each holding its nqc chunks one after
+//    the other:
+//      element (i, a, Q) at ((i*rows/256 + a/256)*nqc + Q/16)*4096
+//                           + ((a%256)/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8
+//    so a 128-row slab of one chunk is 4 KB and a 256-row slab of consecutive
+//    chunks is one contiguous run;
+//  * pair_layout = true (fused pair energies): one array of 128-row blocks
+//    whose chunks hold the hi slab and then the lo slab of the same rows:
+//      hi of (i, a, Q) at ((i*rows/128 + a/128)*nqc + Q/16)*4096
+//                         + ((a%128)/8*16 + (Q%16)/8*8 + a%8)*8 + Q%8,
+//      lo at the same + 2048,
+//    so one contiguous copy brings both halves of a 128-row slab for several
+//    chunks, and each chunk's [hi; lo] is a 256-row operand.
+// rows is a multiple of 256.
 static __global__ void split_fixed_blocked_kernel(const double* __restrict__ src, int64_t vp,
                                                   int64_t Mp, int v, int M, int64_t o, int64_t nqc,
                                                   int64_t rows, const int* __restrict__ expo,
-                                                  uint16_t* __restrict__ hi, uint16_t* __restrict__ lo) {
+                                                  uint16_t* __restrict__ hi, uint16_t* __restrict__ lo,
+                                                  bool pair_layout) {
     // one thread = one core-matrix row: 8 consecutive Q of one a
     const int64_t total = o * nqc * rows * 2;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
@@ -135,14 +147,16 @@ static __global__ void split_fixed_blocked_kernel(const double* __restrict__ src
             h[k] = __half_as_ushort(__double2half(hv));   // exact: |hv| <= 1024
             l[k] = __half_as_ushort(__double2half(lv));   // exact: |lv| <= 128
         }
-        const int64_t off = ((i * (rows / 256) + (g >> 5)) * nqc + qc) * 4096 + ((g & 31) * 16 + kk * 8 + r) * 8;
+        const int64_t off = pair_layout
+                                ? ((i * (rows / 128) + (g >> 4)) * nqc + qc) * 4096 + ((g & 15) * 16 + kk * 8 + r) * 8
+                                : ((i * (rows / 256) + (g >> 5)) * nqc + qc) * 4096 + ((g & 31) * 16 + kk * 8 + r) * 8;
         uint4 vh, vl;
         vh.x = h[0] | (uint32_t(h[1]) << 16); vh.y = h[2] | (uint32_t(h[3]) << 16);
         vh.z = h[4] | (uint32_t(h[5]) << 16); vh.w = h[6] | (uint32_t(h[7]) << 16);
         vl.x = l[0] | (uint32_t(l[1]) << 16); vl.y = l[2] | (uint32_t(l[3]) << 16);
         vl.z = l[4] | (uint32_t(l[5]) << 16); vl.w = l[6] | (uint32_t(l[7]) << 16);
         *reinterpret_cast<uint4*>(hi + off) = vh;
-        *reinterpret_cast<uint4*>(lo + off) = vl;
+        *reinterpret_cast<uint4*>((pair_layout ? hi + 2048 : lo) + off) = vl;
     }
 }
 
