@@ -626,16 +626,16 @@ def bench_gpu(args, w, rank, world, local_rank):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one captured
 # launch of the dominant kernel, with the extent of that launch: the Gamma
-# GEMM of the first block pair of the default step (R = K = 30 occupied
-# orbitals x 1920 padded virtuals, Q = 8192, 30 x 1800 rows of Gamma
+# GEMM of the first block pair of the default step (R = K = 25 occupied
+# orbitals x 1920 padded virtuals, Q = 8192, 25 x 1800 rows of Gamma
 # read-modified-written), captured in one ncu pass with wave pacing and
 # 16-row-block tile groups (profiles/gamma_tc_kernel_cdmp2_grad_n2000_o200_m8000.md).
 # A wave of Gamma tiles reads its operand rows once per K step and a launch
 # has R / 128 * Q / 256 / 148 waves, so the operand traffic of a launch grows
 # as R * K; the read-modify-write of Gamma adds 16 bytes per written element.
 CAPTURED_TRAFFIC = {
-    "gamma_tc_kernel": {"bytes": 83754782976 + 2930398976, "R": 57600, "K": 57600,
-                        "rmw": 16 * 30 * 1800 * 8000},
+    "gamma_tc_kernel": {"bytes": 83795767808 + 2927466240, "R": 48000, "K": 48000,
+                        "rmw": 16 * 25 * 1800 * 8000},
 }
 
 

@@ -62,11 +62,13 @@ constexpr size_t kPartTcBudget = size_t(16) << 30;
 constexpr size_t kPartF64Budget = size_t(8) << 30;
 
 // Wave pacing of the persistent tile kernels (WavePacer in sm100_ptx.cuh):
-// copies per epoch and epochs of slack.  MSHQC_CD_PACE (Gamma) and
-// MSHQC_CD_PACE_TILES (integral tiles) = off disables it, = <every>,<slack>
-// sets both.
-void pace_params(int* every, int* slack, const char* var = "MSHQC_CD_PACE") {
-    *every = 16;
+// copies per epoch and epochs of slack.  On by default for Gamma (its K runs
+// to 57600 and unpaced CTAs drift apart: 7x the DRAM traffic), off for the
+// integral tiles (K = M; pacing them changed nothing at N=2000).
+// MSHQC_CD_PACE (Gamma) and MSHQC_CD_PACE_TILES (integral tiles) = off
+// disables it, = <every>,<slack> enables it with those values.
+void pace_params(int* every, int* slack, const char* var, bool on_by_default) {
+    *every = on_by_default ? 16 : 0;
     *slack = 2;
     const char* env = std::getenv(var);
     if (!env) return;
@@ -1024,7 +1026,7 @@ int launch_gamma(mshqc_cd_ctx* ctx, const uint16_t* ahi, const uint16_t* alo, in
     const int grid = (int)std::min<int64_t>((int64_t)g.nrb * g.nqb, ctx->num_sms);
     g.group = 16;
     if (const char* env = std::getenv("MSHQC_CD_GAMMA_GROUP")) g.group = std::max(1, std::atoi(env));
-    pace_params(&g.pace_every, &g.pace_slack);
+    pace_params(&g.pace_every, &g.pace_slack, "MSHQC_CD_PACE", true);
     if (g.pace_every > 0) {
         CD_ALLOC(ctx->pace, sizeof(int) * (size_t)grid, true);
         g.pace = ctx->pace.as<int>();
@@ -1124,7 +1126,7 @@ int tc_backward_pass(mshqc_cd_ctx* ctx, int sx, int sy, const uint16_t* const bt
             a.tri = tri ? 1 : 0;
             const int64_t vunits = (int64_t)npl * a.nbx * a.nby;
             const int vgrid = (int)std::min<int64_t>(vunits, ctx->num_sms);
-            pace_params(&a.pace_every, &a.pace_slack, "MSHQC_CD_PACE_TILES");
+            pace_params(&a.pace_every, &a.pace_slack, "MSHQC_CD_PACE_TILES", false);
             if (a.pace_every > 0) {
                 CD_ALLOC(ctx->pace, sizeof(int) * (size_t)vgrid, true);
                 a.pace = ctx->pace.as<int>();
