@@ -269,6 +269,21 @@ MSHQC_CD_API int mshqc_cd_set_core_hamiltonian(mshqc_cd_ctx* ctx, const double* 
  * are the rotated orbitals (OMP2Result::C_alpha / C_beta). */
 MSHQC_CD_API int mshqc_cd_get_orbitals(mshqc_cd_ctx* ctx, int spin, double* C, int where);
 
+/* Cholesky Fock build of the SCF classes on the context's vectors (stored or
+ * generated), FP64: J = sum_Q <L^Q, P_tot> L^Q and K_s = sum_Q L^Q P_s L^Q.
+ *  nspin = 1 replaces CholeskyRHF::build_fock (src/scf/cholesky_rhf.cc:99-137):
+ *    P_a is the total density 2 C_occ C_occ^T, F_a = H + J - K_a / 2, and with
+ *    screen_exchange != 0 vectors of Frobenius norm <= 1e-8 are left out of K
+ *    (CholeskyRHFConfig::screen_exchange, default on in the reference);
+ *  nspin = 2 replaces CholeskyUHF::build_fock_cholesky
+ *    (src/scf/cholesky_uhf.cc:77-103): J from P_a + P_b, F_s = H + J - K_s
+ *    (never screened).
+ * All matrices N*N (symmetric, so either storage order).  Every output may be
+ * NULL; a Fock matrix needs H. */
+MSHQC_CD_API int mshqc_cd_cholesky_fock(mshqc_cd_ctx* ctx, int nspin, const double* P_a, const double* P_b,
+                                        const double* H, int screen_exchange, double* F_a, double* F_b,
+                                        double* J, double* K_a, double* K_b, int where);
+
 /* One gradient evaluation of CholeskyOMP2::compute at the context's current
  * alpha and beta orbitals (src/mp2/cholesky_omp2.cc:442-466): amplitudes
  * (:94-183), MP2 energy (:189-230), the one-particle density blocks G_oo

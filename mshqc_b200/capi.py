@@ -95,6 +95,7 @@ SIGNATURES = {
     "mshqc_cd_omp2_pieces": (_i32, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double), _vp, _vp, _vp, _vp,
                                     _vp, _vp, _i32]),
     "mshqc_cd_omp2": (_i32, [_vp, ctypes.POINTER(Omp2Config), _vp, _vp, _i32, ctypes.POINTER(Omp2Result)]),
+    "mshqc_cd_cholesky_fock": (_i32, [_vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _i32]),
     "mshqc_cd_rmp2_energy_noalloc": (_i32, [_vp, _vp, _i64, _i64, _i64, _vp, _vp]),
     "mshqc_cd_get_t2_block": (_i32, [_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i32]),
     "mshqc_cd_set_collectives": (_i32, [_vp, ctypes.POINTER(Collectives)]),
@@ -448,6 +449,25 @@ class Context:
         out["e_mp2"] = e.value
         out["w_a"] = 2.0 * out["F_a"][oa:, :oa]
         out["w_b"] = 2.0 * out["F_b"][ob:, :ob]
+        return out
+
+    def cholesky_fock(self, H, P_a, P_b=None, screen_exchange: bool = True) -> dict:
+        """Cholesky Fock build on the context's vectors: with one density the
+        CholeskyRHF build (P_a the total density, F = H + J - K/2), with two
+        the CholeskyUHF build (F_s = H + J - K_s).  Returns J, K_a, F_a (and
+        K_b, F_b), N x N column-major."""
+        N = self.nbf
+        f = lambda x: np.asfortranarray(x, dtype=np.float64)
+        H, P_a = f(H), f(P_a)
+        nspin = 1 if P_b is None else 2
+        P_b = f(P_b) if P_b is not None else None
+        out = {k: np.empty((N, N), order="F") for k in ("J", "K_a", "F_a")}
+        if nspin == 2:
+            out.update({k: np.empty((N, N), order="F") for k in ("K_b", "F_b")})
+        _check(self._lib.mshqc_cd_cholesky_fock(
+            self._h, nspin, _ptr(P_a), _ptr(P_b) if P_b is not None else None, _ptr(H),
+            1 if screen_exchange else 0, _ptr(out["F_a"]), _ptr(out["F_b"]) if nspin == 2 else None,
+            _ptr(out["J"]), _ptr(out["K_a"]), _ptr(out["K_b"]) if nspin == 2 else None, HOST))
         return out
 
     def omp2(self, max_iterations: int = 50, energy_threshold: float = 1e-6,

@@ -473,6 +473,104 @@ int reference_densities(mshqc_cd_ctx* ctx, const double* Pa, const double* Pb, i
     return MSHQC_CD_OK;
 }
 
+// norm2[q] = sum_k L[q * n + k]^2 (one CTA per q, fixed-order tree)
+__global__ void row_norm2_kernel(const double* __restrict__ L, int64_t n, double* __restrict__ norm2) {
+    __shared__ double red[256];
+    const double* row = L + (int64_t)blockIdx.x * n;
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < n; k += 256) s = fma(row[k], row[k], s);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) norm2[blockIdx.x] = red[0];
+}
+
+// Z^q = 0 for the vectors whose Frobenius norm is at most `thr` (the
+// exchange screening of src/scf/cholesky_rhf.cc:120-126); norm2[q] = |L^q|^2
+__global__ void screen_slabs_kernel(double* __restrict__ Z, const double* __restrict__ norm2, int64_t nn,
+                                    double thr) {
+    if (norm2[blockIdx.y] > thr * thr) return;
+    double* z = Z + (int64_t)blockIdx.y * nn;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn; t += (int64_t)gridDim.x * blockDim.x)
+        z[t] = 0.0;
+}
+
+// Cholesky Coulomb and exchange matrices of the SCF Fock builds,
+//   J = sum_Q <L^Q, P_tot> L^Q,   K_s = sum_Q L^Q P_s L^Q,
+// P_tot = P[0] (nspin 1) or P[0] + P[1] (nspin 2), over chunks of vectors
+// (stored or generated): per chunk the coefficients <L^Q, P_tot> (one dot
+// product per vector), J += coef . L as one GEMM, Z^Q = P_s L^Q as one batched
+// GEMM and K_s += L . Z as one GEMM over the composite index (Q, nu).  All
+// matrices are N x N and symmetric; device pointers on the context stream.
+int cholesky_jk_device(mshqc_cd_ctx* ctx, int nspin, const double* const P[2], bool screen, double* J,
+                       double* const K[2], double* work) {
+    const int64_t N = ctx->N, NN = N * N, M = ctx->M;
+    const double* Ptot = P[0];
+    if (nspin == 2) {
+        axpy_kernel<<<blocks_for(NN), 256, 0, ctx->stream>>>(P[0], 1.0, P[1], NN, work);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+        Ptot = work;
+    }
+    CD_CUDA(cudaMemsetAsync(J, 0, sizeof(double) * NN, ctx->stream));
+    for (int s = 0; s < nspin; ++s) CD_CUDA(cudaMemsetAsync(K[s], 0, sizeof(double) * NN, ctx->stream));
+    // vectors per chunk: the generator's chunk, and at most 2 GB of Z
+    const int64_t mc_max = std::max<int64_t>(
+        1, std::min<int64_t>({vectors_chunk_size(ctx), (int64_t)((size_t(2) << 30) / (sizeof(double) * NN)),
+                              (int64_t)65535}));
+    CD_ALLOC(ctx->Zt, sizeof(double) * (size_t)(mc_max * NN), false);
+    CD_ALLOC(ctx->omp2_ws, sizeof(double) * (size_t)(2 * mc_max), false);
+    double* coef = ctx->omp2_ws.as<double>();
+    double* norm2 = coef + mc_max;
+    for (int64_t Q0 = 0; Q0 < M; Q0 += mc_max) {
+        const int64_t mc = std::min<int64_t>(mc_max, M - Q0);
+        const double* Lc = nullptr;
+        CD_RC(vectors_chunk(ctx, Q0, mc, &Lc));
+        dot_rows_kernel<<<(unsigned)mc, 256, 0, ctx->stream>>>(Lc, NN, Ptot, coef);
+        CD_CUDA(cudaGetLastError());
+        ctx->launches++;
+        GemmF64Args g{};
+        g.M = 1;  g.N = (int)NN;  g.K = (int)mc;  g.batch = 1;
+        g.A = coef;  g.lda = mc;  g.B = Lc;  g.ldb = NN;  g.C = J;  g.ldc = NN;
+        g.alpha = 1.0;  g.beta = 1.0;
+        CD_CUDA(gemm_f64(g, true, false, ctx->stream));
+        ctx->launches++;
+        if (screen) {
+            row_norm2_kernel<<<(unsigned)mc, 256, 0, ctx->stream>>>(Lc, NN, norm2);
+            CD_CUDA(cudaGetLastError());
+            ctx->launches++;
+        }
+        for (int s = 0; s < nspin; ++s) {
+            GemmF64Args z{};
+            z.M = (int)N;  z.N = (int)N;  z.K = (int)N;  z.batch = (int)mc;
+            z.A = P[s];  z.lda = N;  z.sA = 0;
+            z.B = Lc;  z.ldb = N;  z.sB = NN;
+            z.C = ctx->Zt.as<double>();  z.ldc = N;  z.sC = NN;
+            z.alpha = 1.0;  z.beta = 0.0;
+            CD_CUDA(gemm_f64(z, true, false, ctx->stream));
+            ctx->launches++;
+            if (screen) {
+                dim3 grid((unsigned)std::min<int64_t>(cdiv(NN, 256), 1024), (unsigned)mc);
+                screen_slabs_kernel<<<grid, 256, 0, ctx->stream>>>(ctx->Zt.as<double>(), norm2, NN, 1e-8);
+                CD_CUDA(cudaGetLastError());
+                ctx->launches++;
+            }
+            GemmF64Args k{};
+            k.M = (int)N;  k.N = (int)N;  k.K = (int)(mc * N);  k.batch = 1;
+            k.A = Lc;  k.lda = N;
+            k.B = ctx->Zt.as<double>();  k.ldb = N;
+            k.C = K[s];  k.ldc = N;
+            k.alpha = 1.0;  k.beta = 1.0;
+            CD_CUDA(gemm_f64(k, false, false, ctx->stream));
+            ctx->launches++;
+        }
+    }
+    return MSHQC_CD_OK;
+}
+
 }  // namespace
 }  // namespace mshqc_cd
 
@@ -620,6 +718,61 @@ MSHQC_CD_API int mshqc_cd_omp2(mshqc_cd_ctx* ctx, const mshqc_cd_omp2_config* cf
     res->iterations = iter;
     res->converged = converged;
     res->ms_total = ms;
+    return MSHQC_CD_OK;
+}
+
+MSHQC_CD_API int mshqc_cd_cholesky_fock(mshqc_cd_ctx* ctx, int nspin, const double* P_a, const double* P_b,
+                                        const double* H, int screen_exchange, double* F_a, double* F_b,
+                                        double* J, double* K_a, double* K_b, int where) {
+    if (!ctx) return set_error(MSHQC_CD_ERR_ARG, "null context");
+    if (nspin != 1 && nspin != 2) return set_error(MSHQC_CD_ERR_ARG, "nspin must be 1 (RHF) or 2 (UHF)");
+    if (!P_a || (nspin == 2 && !P_b)) return set_error(MSHQC_CD_ERR_ARG, "density missing");
+    if ((F_a || (nspin == 2 && F_b)) && !H) return set_error(MSHQC_CD_ERR_ARG, "a Fock matrix needs H");
+    if (where != MSHQC_CD_HOST && where != MSHQC_CD_DEVICE) return set_error(MSHQC_CD_ERR_ARG, "bad where");
+    if (!ctx->L_set) return set_error(MSHQC_CD_ERR_STATE, "set_vectors (or gen_vectors) must come first");
+    DeviceGuard g(ctx->device);
+    reset_stages(ctx);
+    const int64_t NN = ctx->N * ctx->N;
+    // P_a P_b H | J K_a K_b | F work
+    CD_ALLOC(ctx->opdm, sizeof(double) * (size_t)(8 * NN), false);
+    double* base = ctx->opdm.as<double>();
+    double* P[2] = {base, base + NN};
+    double* Hd = base + 2 * NN;
+    double* Jd = base + 3 * NN;
+    double* Kd[2] = {base + 4 * NN, base + 5 * NN};
+    double* Fd = base + 6 * NN;
+    double* work = base + 7 * NN;
+    const double* in[3] = {P_a, nspin == 2 ? P_b : nullptr, H};
+    double* dst[3] = {P[0], P[1], Hd};
+    for (int k = 0; k < 3; ++k) {
+        if (!in[k]) continue;
+        if (where == MSHQC_CD_HOST)
+            CD_RC(upload(ctx, dst[k], in[k], sizeof(double) * NN));
+        else
+            CD_CUDA(cudaMemcpyAsync(dst[k], in[k], sizeof(double) * NN, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    const double* Pc[2] = {P[0], P[1]};
+    begin_stage(ctx, ST_OTHER);
+    CD_RC(cholesky_jk_device(ctx, nspin, Pc, nspin == 1 && screen_exchange != 0, Jd, Kd, work));
+    end_stage(ctx);
+    if (J) CD_RC(download(ctx, J, Jd, sizeof(double) * NN, where));
+    double* Kout[2] = {K_a, K_b};
+    double* Fout[2] = {F_a, F_b};
+    // RHF (src/scf/cholesky_rhf.cc:136): F = H + J - K/2 with the total density;
+    // UHF (src/scf/cholesky_uhf.cc:90-98): F_s = H + J - K_s
+    const double kf = nspin == 1 ? -0.5 : -1.0;
+    for (int s = 0; s < nspin; ++s) {
+        if (Kout[s]) CD_RC(download(ctx, Kout[s], Kd[s], sizeof(double) * NN, where));
+        if (Fout[s]) {
+            axpy_kernel<<<blocks_for(NN), 256, 0, ctx->stream>>>(Hd, 1.0, Jd, NN, Fd);
+            axpy_kernel<<<blocks_for(NN), 256, 0, ctx->stream>>>(Fd, kf, Kd[s], NN, Fd);
+            CD_CUDA(cudaGetLastError());
+            ctx->launches += 2;
+            CD_RC(download(ctx, Fout[s], Fd, sizeof(double) * NN, where));
+        }
+    }
+    CD_CUDA(cudaStreamSynchronize(ctx->stream));
+    collect_stages(ctx);
     return MSHQC_CD_OK;
 }
 

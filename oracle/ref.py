@@ -46,6 +46,7 @@ def _load():
         lib.ref_cholesky_decompose.argtypes = [i, _dp, d, i, _dp, _ip]
         lib.ref_omp2_mp2_part.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, i, i, i, _dp]
         lib.ref_rhf_cdrmp2.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, d, d, d, i, _dp, _dp, _dp, _ip]
+        lib.ref_cholesky_fock.argtypes = [i, i, _dp, i, _dp, _dp, _dp, i, _dp, _dp]
         _lib = lib
     return _lib
 
@@ -191,3 +192,26 @@ def cholesky_decompose(eri, threshold):
     m = ctypes.c_int(0)
     _check(lib.ref_cholesky_decompose(N, _p(E), threshold, cap, _p(Lout), ctypes.byref(m)))
     return Lout[: m.value].copy()
+
+
+def cholesky_fock(L, H, Pa, Pb=None, screen_exchange=True):
+    """The reference's Cholesky Fock build on vectors L (M, N*N): with one
+    density the CholeskyRHF build (src/scf/cholesky_rhf.cc:99-137,
+    F = H + J - K/2, P the total density), with two the CholeskyUHF build
+    (src/scf/cholesky_uhf.cc:77-103, F_s = H + J - K_s).  Returns F or
+    (F_a, F_b), column-major N x N arrays."""
+    lib = _load()
+    L = np.ascontiguousarray(L, dtype=np.float64)
+    M, nn = L.shape
+    N = int(round(nn ** 0.5))
+    f = lambda x: np.asfortranarray(x, dtype=np.float64)
+    H, Pa = f(H), f(Pa)
+    Pb_ = f(Pb) if Pb is not None else Pa
+    Fa = np.zeros((N, N), order="F")
+    Fb = np.zeros((N, N), order="F")
+    ptr = lambda a: a.ctypes.data_as(_dp)
+    rc = lib.ref_cholesky_fock(N, M, ptr(L), 1 if Pb is None else 2, ptr(Pa), ptr(Pb_), ptr(H),
+                               1 if screen_exchange else 0, ptr(Fa), ptr(Fb))
+    if rc != 0:
+        raise RuntimeError(lib.ref_last_error().decode())
+    return Fa if Pb is None else (Fa, Fb)

@@ -6,6 +6,7 @@
 //   CholeskyUMP2   src/mp2/cholesky_ump2.cc
 //   CholeskyOMP2   src/mp2/cholesky_omp2.cc
 //   CholeskyERI    src/integrals/cholesky_eri.cc
+//   CholeskyRHF / CholeskyUHF Fock builds  src/scf/cholesky_{rhf,uhf}.cc
 // Tests and bench.py's reference arm call it through ctypes (oracle/ref.py)
 // to pin the CPU restatement and to time the reference CPU path.
 //
@@ -36,7 +37,9 @@
 #define protected public
 #include "mshqc/basis.h"
 #include "mshqc/cholesky_omp2.h"
+#include "mshqc/cholesky_rhf.h"
 #include "mshqc/cholesky_rmp2.h"
+#include "mshqc/cholesky_uhf.h"
 #include "mshqc/cholesky_ump2.h"
 #include "mshqc/integrals.h"
 #include "mshqc/integrals/cholesky_eri.h"
@@ -375,6 +378,60 @@ int ref_rhf_cdrmp2(int N, int natom, const double* Z, const double* xyz, const d
     } catch (const std::exception& ex) {
         g_err = ex.what();
         oracle_stub::g_have_eri = false;
+        return -1;
+    }
+}
+
+// One Cholesky Fock build of the reference's SCF classes on given vectors,
+// core Hamiltonian and densities (N x N, column-major):
+//   nspin = 1: CholeskyRHF::build_fock (src/scf/cholesky_rhf.cc:99-137),
+//              F = H + J - 0.5 K with P the total density, K screened when
+//              screen != 0 (vectors of norm <= 1e-8 skipped);
+//   nspin = 2: CholeskyUHF::build_fock_cholesky (src/scf/cholesky_uhf.cc:77-103),
+//              F_s = H + J[P_a + P_b] - K[P_s].
+int ref_cholesky_fock(int N, int M, const double* L, int nspin, const double* Pa, const double* Pb,
+                      const double* H, int screen, double* Fa, double* Fb) {
+    try {
+        Quiet q(true);
+        const Eigen::Map<const Eigen::MatrixXd> Hm(H, N, N);
+        if (nspin == 1) {
+            integrals::CholeskyERI chol(1e-6);
+            fill_cholesky(chol, N, M, L);
+            Molecule mol;
+            mol.add_atom(2, 0.0, 0.0, 0.0);   // any closed shell: the Fock build reads no electron count
+            BasisSet basis = make_basis(N);
+            auto ints = std::make_shared<IntegralEngine>(mol, basis);
+            CholeskyRHFConfig cfg;
+            cfg.print_level = 0;
+            cfg.screen_exchange = screen != 0;
+            CholeskyRHF rhf(mol, basis, ints, cfg, chol);
+            rhf.H_ = Hm;
+            rhf.P_ = Eigen::Map<const Eigen::MatrixXd>(Pa, N, N);
+            rhf.build_fock();
+            std::memcpy(Fa, rhf.F_.data(), sizeof(double) * (size_t)N * N);
+            return 0;
+        }
+        Molecule mol;
+        mol.add_atom(2, 0.0, 0.0, 0.0);
+        BasisSet basis = make_basis(N);
+        auto ints = std::make_shared<IntegralEngine>(mol, basis);
+        CholeskyUHFConfig cfg;
+        cfg.print_level = 0;
+        CholeskyUHF uhf(mol, basis, ints, 1, 1, cfg);
+        const size_t nn = static_cast<size_t>(N) * N;
+        std::vector<Eigen::VectorXd> vecs;
+        vecs.reserve(M);
+        for (int k = 0; k < M; ++k) vecs.push_back(Eigen::Map<const Eigen::VectorXd>(L + k * nn, nn));
+        uhf.set_cholesky_vectors(vecs);
+        uhf.H_ = Hm;
+        uhf.P_a_ = Eigen::Map<const Eigen::MatrixXd>(Pa, N, N);
+        uhf.P_b_ = Eigen::Map<const Eigen::MatrixXd>(Pb, N, N);
+        uhf.build_fock_cholesky();
+        std::memcpy(Fa, uhf.F_a_.data(), sizeof(double) * nn);
+        std::memcpy(Fb, uhf.F_b_.data(), sizeof(double) * nn);
+        return 0;
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
         return -1;
     }
 }
