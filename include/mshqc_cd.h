@@ -61,12 +61,14 @@ enum mshqc_cd_precision {
                              FP16, three products per pair, exact FP32
                              accumulation on the tensor cores; FP64
                              denominators, diagonal integrals and energies;
-                             the half transforms and the backward's
+                             the half transforms (from nbf = 512 on;
+                             below, FP64 DMMA) and the backward's
                              transposed transforms as FP64 products of
                              int8 slices (5 x 7 bits per operand row) on
                              the tensor cores, about 2^-32 of the row
                              maxima per term (MSHQC_CD_TRANSFORM=f64 in the
-                             environment: FP64 DMMA instead)             */
+                             environment: FP64 DMMA for both, =i8: int8
+                             slices for both at every size)              */
 };
 
 enum mshqc_cd_kind {
@@ -108,7 +110,7 @@ MSHQC_CD_API int mshqc_cd_set_stream(mshqc_cd_ctx* ctx, void* stream);
 /* Share one gradient among nranks contexts, one per GPU (no counterpart in
  * the reference, which runs on one node): mshqc_cd_mp2_gradient of this
  * context then computes its share of the backward's units (block pairs of
- * occupied orbitals; occupied blocks on the FP64 path) and returns that
+ * occupied orbitals, on the mixed and the FP64 path) and returns that
  * share's energy, dE/dC and dE/deps.  Their sums over the ranks (one
  * all-reduce of 3 + 2 N^2 + 2 N doubles at most) are the full result.
  * The shares: with nranks > 1 the occupied block sizes depend only on the

@@ -230,6 +230,20 @@ bool int8_transform_enabled(const mshqc_cd_ctx* ctx) {
     return !(env && std::strcmp(env, "f64") == 0);
 }
 
+// The forward half transform of a mixed request runs on the int8 tensor
+// cores from N = 512 on; below, the FP64 DMMA products are faster (forward
+// transform of the gradient step, one box: N=400 1.8 ms FP64 vs 2.6 ms int8,
+// N=600 8.8 vs 7.6 ms) and their B is exact.  The transposed transforms keep
+// the int8 products at every size (N=400: 3.4 vs 6.8 ms).
+// MSHQC_CD_TRANSFORM=i8 forces the int8 products, =f64 the FP64 ones.
+constexpr int64_t kInt8ForwardMinN = 512;
+bool int8_forward_enabled(const mshqc_cd_ctx* ctx) {
+    if (!int8_transform_enabled(ctx)) return false;
+    const char* env = std::getenv("MSHQC_CD_TRANSFORM");
+    if (env && std::strcmp(env, "i8") == 0) return true;
+    return ctx->N >= kInt8ForwardMinN;
+}
+
 // The same half transform as transform_f64 with both products on the int8
 // tensor cores (ozaki_i8.cuh): Y = C_occ^T L per vectors chunk, then
 // B_i = C_vir^T Y_i^T in batches of occupied orbitals.  Accuracy of the
@@ -646,7 +660,7 @@ int ensure_transform(mshqc_cd_ctx* ctx, int spin, int precision, int layout) {
         // shared over ranks: this rank's orbitals, then the gather of all
         int64_t lo = 0, hi = s.nocc;
         shard_range(ctx, s.nocc, &lo, &hi);
-        if (precision == MSHQC_CD_FP16X3 && int8_transform_enabled(ctx))
+        if (precision == MSHQC_CD_FP16X3 && int8_forward_enabled(ctx))
             CD_RC(transform_i8(ctx, spin, lo, hi));
         else
             CD_RC(transform_f64(ctx, spin, lo, hi));

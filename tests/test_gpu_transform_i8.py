@@ -7,7 +7,9 @@ The slice products carry an error of about 2^-31 of (row max x row max) per
 term, so the transformed vectors agree with the FP64 ones to
 REL_TOL = 2e-8 of max |B| (the FP64 path: 1e-13).  An FP64 request after a
 mixed one recomputes the vectors in FP64; MSHQC_CD_TRANSFORM=f64 sends the
-mixed path through the FP64 transform.
+mixed path through the FP64 transform, =i8 (set for every test here: these
+sizes are below N = 512, where the library itself switches the forward
+transform to the int8 products) through the int8 one.
 """
 import numpy as np
 import pytest
@@ -19,6 +21,14 @@ from oracle import cdmp2_oracle as orc
 pytestmark = pytest.mark.gpu
 
 REL_TOL = 2e-8
+
+
+@pytest.fixture(autouse=True)
+def int8_forward(monkeypatch):
+    """These sizes are below the one from which the library takes the int8
+    forward transform by itself: force it (tests that switch it off set
+    MSHQC_CD_TRANSFORM=f64 over this)."""
+    monkeypatch.setenv("MSHQC_CD_TRANSFORM", "i8")
 
 
 @pytest.fixture(scope="module")
@@ -115,6 +125,8 @@ def test_mixed_gradient_int8_transposed_vs_fp64(ctx, monkeypatch, switch):
     g64 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP64)
     if switch:
         monkeypatch.setenv("MSHQC_CD_TRANSFORM", switch)
+    else:
+        monkeypatch.delenv("MSHQC_CD_TRANSFORM")      # the library's own choice at this size
     ctx.set_orbitals(capi.ALPHA, a.C, a.eps, o)
     g3 = ctx.mp2_gradient(capi.RESTRICTED, capi.FP16X3)
     assert abs(g3.energy["total"] - g64.energy["total"]) <= 1e-6
